@@ -1,0 +1,248 @@
+/*
+ * mpf.h — C-ABI of the B200-native batched AC power-flow engine (libmpf.so).
+ *
+ * One handle = one grid (buses + branches) with its symbolic analysis done
+ * once on the host, plus a batch of cases.  A case is the base grid with a
+ * set of outaged branches (N-1, N-k) and, optionally, its own bus
+ * injections (load scenarios).  mpf_solve runs Newton-Raphson or
+ * fast-decoupled XB/BX over every case of the batch on one GPU.
+ *
+ * This replaces the reference's power-flow entry points:
+ *   hybrid_init  (src/powerflow/runpf.h:795)  -> mpf_create + mpf_set_cases
+ *   hybrid_runpf (src/powerflow/runpf.h:606)  -> mpf_solve (+ mpf_get_results)
+ *   hybrid_free  (src/powerflow/runpf.h:984)  -> mpf_destroy
+ *   mkl_runpf    (src/powerflow/runpf.h:259)  -> mpf_runpf_host (host buffers in/out)
+ * and the algorithm constants NR/FDXB/FDBX (src/powerflow/runpf.h:16-18),
+ * MAX_IT_NR/MAX_IT_FD/EPS (src/powerflow/runpf.h:45-47).
+ *
+ * Conventions follow the reference data model:
+ *   bus.p, bus.q   net injection (generation - demand) in p.u.   (Bus.h:27-28,
+ *                  files/loadMatpowerFormat.h:87-88,120-123)
+ *   bus.va         voltage angle in radians                       (loadMatpowerFormat.h:87)
+ *   branch.tap     off-nominal ratio, 0 means "no transformer" -> 1 (makeYbus.h:332)
+ *   branch.shift   phase shift in degrees                         (makeYbus.h:333-335)
+ *   J ordering     rows [P_pv, P_pq, Q_pq], cols [Va_pv, Va_pq, Vm_pq], PV and PQ
+ *                  buses in bus-index order                       (Topology.h:100-126)
+ *
+ * Errors never exit or trap: every entry point returns an mpf_status and
+ * mpf_last_error() gives a message.  Per-case outcomes are mpf_case_status.
+ */
+#ifndef MPF_H_
+#define MPF_H_
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPF_ABI_VERSION 1
+
+/* algorithms — same values as NR / FDXB / FDBX in src/powerflow/runpf.h:16-18 */
+#define MPF_NR   0
+#define MPF_FDXB 1
+#define MPF_FDBX 2
+
+/* precision of the LU factorisation and triangular solves (mismatch, update and
+ * convergence test are always FP64) */
+#define MPF_FP64  0
+#define MPF_MIXED 1
+
+/* defaults — MAX_IT_NR, MAX_IT_FD, EPS in src/powerflow/runpf.h:45-47 */
+#define MPF_DEFAULT_MAX_IT_NR 10
+#define MPF_DEFAULT_MAX_IT_FD 30
+#define MPF_DEFAULT_TOL 1e-8
+
+/* bus types — Bus::Type in src/powersystem/Bus.h:11-13 (MATPOWER codes) */
+#define MPF_BUS_NONE     0
+#define MPF_BUS_PQ       1
+#define MPF_BUS_PV       2
+#define MPF_BUS_SLACK    3
+#define MPF_BUS_ISOLATED 4
+
+typedef enum mpf_status {
+  MPF_OK = 0,
+  MPF_ERR_BAD_INPUT = 1,   /* invalid argument or grid */
+  MPF_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  MPF_ERR_OOM = 3,         /* device or host allocation failed */
+  MPF_ERR_STATE = 4,       /* call out of order (e.g. solve before set_cases) */
+  MPF_ERR_TIMEOUT = 5,     /* a bounded device-side wait ran out */
+  MPF_ERR_INTERNAL = 6,
+  MPF_ERR_NO_DEVICE = 7    /* no CUDA device visible */
+} mpf_status;
+
+typedef enum mpf_case_status {
+  MPF_CASE_RUNNING = 0,    /* not finished (only seen mid-solve) */
+  MPF_CASE_CONVERGED = 1,  /* max |mismatch| < tol */
+  MPF_CASE_MAX_ITER = 2,   /* iteration limit reached (the reference's "not converged") */
+  MPF_CASE_DIVERGED = 3,   /* non-finite mismatch or voltage */
+  MPF_CASE_SINGULAR = 4    /* zero / tiny pivot in the LU */
+} mpf_case_status;
+
+/* Bus record: the fields of Bus (src/powersystem/Bus.h:18-31) the power flow reads. */
+typedef struct mpf_bus {
+  int32_t type;   /* MPF_BUS_* */
+  int32_t pad_;
+  double vm;      /* voltage magnitude (p.u.); PV/slack: set-point */
+  double va;      /* voltage angle (radians) */
+  double p;       /* net active injection (p.u.) */
+  double q;       /* net reactive injection (p.u.) */
+  double gsh;     /* shunt conductance (p.u.) */
+  double bsh;     /* shunt susceptance (p.u.) */
+} mpf_bus;
+
+/* Branch record: the fields of Branch (src/powersystem/Branch.h:18-26). */
+typedef struct mpf_branch {
+  int32_t from;   /* 0-based bus index */
+  int32_t to;
+  int32_t status; /* 1 in service, 0 out of service (Branch::inservice) */
+  int32_t pad_;
+  double r, x, b; /* series R, X and total line charging B (p.u.) */
+  double tap;     /* ratio; 0 = no transformer (treated as 1) */
+  double shift;   /* degrees */
+} mpf_branch;
+
+typedef struct mpf_options {
+  int32_t max_it_nr;   /* default 10 */
+  int32_t max_it_fd;   /* default 30 */
+  double tol;          /* default 1e-8 p.u., strict '<' on max |F| */
+  int32_t angle_mode;  /* 0: atan2 (default); 1: atan(y/x) as cuCangle in
+                          src/util/complexUtils.h:21-23 (loses the quadrant) */
+  int32_t device;      /* CUDA device ordinal, default 0 */
+  int32_t use_graph;   /* 1: capture the Newton iteration in a CUDA graph (default 1) */
+  int32_t reserved[5];
+} mpf_options;
+
+/* Per-kernel device time of the last mpf_solve (CUDA events on the solve stream),
+ * milliseconds, summed over all launches of that kernel in the solve. */
+typedef struct mpf_timing {
+  double total_ms;
+  double mismatch_ms, jacobian_ms, factor_ms, solve_ms, update_ms, other_ms;
+  int32_t iterations_max;   /* max iterations over cases */
+  int32_t launches;         /* kernels launched by the last solve */
+} mpf_timing;
+
+/* Symbolic statistics of the handle (for reports and tests). */
+typedef struct mpf_stats {
+  int32_t n_bus, n_branch, n_pv, n_pq, n_slack;
+  int32_t nnz_ybus;
+  int32_t n_jac, nnz_jac, nnz_lu, lu_levels;   /* Newton system */
+  int64_t lu_flops;                            /* multiply-adds x2 per factorisation */
+  int32_t n_bp, nnz_bp_lu, bp_levels;          /* B' system */
+  int32_t n_bpp, nnz_bpp_lu, bpp_levels;       /* B'' system */
+  int32_t n_cases, case_groups;
+  int64_t device_bytes;                        /* device memory held by the handle */
+} mpf_stats;
+
+typedef struct mpf_handle mpf_handle;
+
+/* ---- library ---------------------------------------------------------- */
+int32_t mpf_abi_version(void);
+void mpf_default_options(mpf_options* opt);
+const char* mpf_status_string(int32_t status);
+
+/* ---- handle lifecycle (replaces hybrid_init / hybrid_free) ------------- */
+/* Validates the grid, builds the superset Ybus pattern, the Jacobian, B' and B''
+ * patterns, their fill-reducing orderings and symbolic LU, and uploads the shared
+ * (case-independent) arrays to the device.  Exactly one slack bus is required. */
+int32_t mpf_create(const mpf_bus* buses, int32_t n_bus,
+                   const mpf_branch* branches, int32_t n_branch,
+                   const mpf_options* opt, mpf_handle** out);
+int32_t mpf_destroy(mpf_handle* h);
+const char* mpf_last_error(const mpf_handle* h);
+int32_t mpf_get_stats(const mpf_handle* h, mpf_stats* st);
+
+/* ---- cases ------------------------------------------------------------- */
+/* Defines the batch.  Case c outages branches
+ *   outage_branches[outage_offsets[c] .. outage_offsets[c+1]-1]
+ * (outage_offsets has n_cases+1 entries; both may be NULL for n_cases base cases).
+ * sbus (nullable): per-case net injections, [n_cases][n_bus][2] (p, q) in p.u.;
+ * NULL means every case uses the grid's bus.p / bus.q.
+ * All pointers are host pointers; the data is copied. */
+int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases,
+                      const int32_t* outage_offsets, const int32_t* outage_branches,
+                      const double* sbus);
+
+/* ---- solve (replaces hybrid_runpf) ------------------------------------- */
+/* Runs alg (MPF_NR / MPF_FDXB / MPF_FDBX) at precision (MPF_FP64 / MPF_MIXED) over
+ * every case, from the reference's start point (runpf.h:211-226: V = vm e^{j va},
+ * PV/slack magnitude = set-point).  stream is a cudaStream_t (NULL = the handle's
+ * own stream).  Asynchronous with respect to the host except for the first call
+ * per (alg, precision), which may synchronise.  Results stay on the device until
+ * read with mpf_get_results / mpf_get_results_device. */
+int32_t mpf_solve(mpf_handle* h, int32_t alg, int32_t precision, void* stream);
+
+/* Blocking copy of the results of the last solve into host buffers (each may be NULL):
+ *   v          [n_cases][n_bus][2]  rectangular voltage (re, im)
+ *   iterations [n_cases]            NR iterations, or FD iterations (P half-steps)
+ *   status     [n_cases]            mpf_case_status
+ *   max_mis    [n_cases]            final max |F| (p.u.)                          */
+int32_t mpf_get_results(mpf_handle* h, double* v, int32_t* iterations,
+                        uint8_t* status, double* max_mis);
+
+/* Same, into device buffers, enqueued on stream (no host synchronisation). */
+int32_t mpf_get_results_device(mpf_handle* h, double* v, int32_t* iterations,
+                               uint8_t* status, double* max_mis, void* stream);
+
+/* One call end to end from host memory, as mkl_runpf / hybrid_runpf are used by
+ * their caller: copies the case definition from host buffers, solves, and copies
+ * the results back into host buffers (each output may be NULL).  Blocking. */
+int32_t mpf_runpf_host(mpf_handle* h, int32_t alg, int32_t precision,
+                       int32_t n_cases, const int32_t* outage_offsets,
+                       const int32_t* outage_branches, const double* sbus,
+                       double* v, int32_t* iterations, uint8_t* status,
+                       double* max_mis);
+
+/* Device time per kernel family of the last solve (synchronises the solve stream). */
+int32_t mpf_get_timing(mpf_handle* h, mpf_timing* t);
+
+/* ---- synthetic inputs (no counterpart in the reference; the reference reads
+ *      MATPOWER files, src/files/loadMatpowerFormat.h:14) --------------------- */
+typedef struct mpf_synth_params {
+  int32_t n_bus;
+  int32_t n_branch;       /* total branches: spanning tree + (n_branch - n_bus + 1) extras */
+  int32_t n_pv;           /* PV buses (plus one slack) */
+  int32_t topology;       /* 0: geometrically local extras; 1: uniform-random extras (stress) */
+  double tap_fraction;    /* fraction of branches with a tap ratio */
+  double tap_lo, tap_hi;  /* tap ~ U(tap_lo, tap_hi) */
+  double r_lo, r_hi;      /* r ~ U(r_lo, r_hi) */
+  double xr_lo, xr_hi;    /* x = r * U(xr_lo, xr_hi) */
+  double b_hi;            /* b ~ U(0, b_hi) */
+  double vset_lo, vset_hi;/* PV/slack |V| set-point ~ U(lo, hi) */
+  double pload_hi;        /* PQ load P ~ U(0, pload_hi) */
+  double qp_lo, qp_hi;    /* Q = P * U(qp_lo, qp_hi) */
+  double gen_factor;      /* PV generation sums to gen_factor * total load */
+  double loading;         /* loading level: drawn loads (P and Q) are multiplied by it */
+  uint64_t seed;
+} mpf_synth_params;
+
+/* Fills params with the distributions shared by all synthetic workloads
+ * (r ~ U(0.01,0.10), x = r U(2,6), b ~ U(0,0.05), |V|set ~ U(1.00,1.06),
+ *  P ~ U(0,0.5), Q = P U(0.2,0.5), generation 1.02 x load, taps U(0.95,1.05))
+ * and loading = 0.2: with these line impedances the unscaled loads leave the base
+ * case without a power-flow solution (loadability 0.2-0.3 at 300+ buses). */
+void mpf_synth_default(mpf_synth_params* p);
+
+/* Deterministic (seeded) synthetic grid; buses[n_bus], branches[n_branch] are caller-owned. */
+int32_t mpf_synth_grid(const mpf_synth_params* p, mpf_bus* buses, mpf_branch* branches);
+
+/* Marks bridges (branches whose removal disconnects the in-service graph):
+ * is_bridge[n_branch] = 1 / 0.  Out-of-service branches are never bridges. */
+int32_t mpf_find_bridges(const mpf_branch* branches, int32_t n_branch, int32_t n_bus,
+                         uint8_t* is_bridge);
+
+/* Picks n_out distinct in-service non-bridge branches in a seeded random order. */
+int32_t mpf_select_outages(const mpf_branch* branches, int32_t n_branch, int32_t n_bus,
+                           int32_t n_out, uint64_t seed, int32_t* out);
+
+/* Load scenarios: sbus[n_cases][n_bus][2] where every bus with a load (p < 0)
+ * gets p, q scaled by (1 + N(0, sigma^2)) (fixed power factor); generation unchanged. */
+int32_t mpf_synth_load_scenarios(const mpf_bus* buses, int32_t n_bus, int32_t n_cases,
+                                 double sigma, uint64_t seed, double* sbus);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPF_H_ */

@@ -1,0 +1,924 @@
+// Host side of libmpf: the handle, device uploads, level schedules, the Newton and
+// fast-decoupled solve loops, and the C-ABI declared in include/mpf.h.
+//
+// Reference counterparts: hybrid_init (src/powerflow/runpf.h:795-982) allocates
+// per-case copies of every sparse structure and creates one CUDA stream per case;
+// hybrid_runpf (runpf.h:606-793) launches one small kernel per case per stage and
+// solves the Newton systems on the host with MKL DSS (newtonpf.h:1086-1158).  Here
+// one handle owns all device memory, every stage is one launch over all cases, and
+// the linear systems are factorised on the device by k_mf_factor.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "internal.h"
+#include "kernels.cuh"
+#include "mpf.h"
+
+using namespace mpf;
+using namespace mpfk;
+
+namespace {
+
+// ------------------------------------------------------------------ errors
+struct MpfError {
+  int code;
+  std::string msg;
+};
+
+#define CUDA_TRY(expr)                                                                     \
+  do {                                                                                     \
+    cudaError_t e_ = (expr);                                                               \
+    if (e_ != cudaSuccess) {                                                               \
+      throw MpfError{e_ == cudaErrorMemoryAllocation ? MPF_ERR_OOM : MPF_ERR_CUDA,        \
+                     std::string(#expr) + ": " + cudaGetErrorString(e_)};                  \
+    }                                                                                      \
+  } while (0)
+
+// ------------------------------------------------------------------ device buffers
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t b) {
+    release();
+    if (b == 0) b = 16;
+    CUDA_TRY(cudaMalloc(&p, b));
+    bytes = b;
+  }
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+template <class T>
+void upload(DevBuf& b, const std::vector<T>& v) {
+  b.alloc(v.size() * sizeof(T));
+  if (!v.empty()) CUDA_TRY(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+
+// ------------------------------------------------------------------ LU system
+enum TaskClass { CLS_S = 0, CLS_M = 1, CLS_L = 2 };
+constexpr int kFmaxS = 8, kFmaxM = 24, kFmaxL = 83;
+
+struct Launch {
+  int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
+};
+
+struct LUSystem {
+  LUSymbolic sym;
+  DevBuf sn_c0, sn_f, sn_rptr, sn_rows, child_ptr, child_list, sn_parent, rel_ptr, relmap, ah_ptr, ah_loc;
+  DevBuf pan_off, cb_off, cbr_off, lev_sn;
+  std::vector<Launch> factor_sched;  // ascending levels
+  std::vector<Launch> level_sched;   // one launch per level (solves), ascending
+  int nA = 0;
+  // values per precision [0] = FP64, [1] = FP32
+  DevBuf A[2], pan[2], cb[2], cbr[2], x[2];
+  int ngroups_alloc[2] = {0, 0};
+
+  DevLU dev() const {
+    DevLU d;
+    d.n = sym.n;
+    d.nsn = sym.nsn;
+    d.nA = nA;
+    d.nnz = sym.nnz;
+    d.sumcb = sym.sum_cb;
+    d.sumcbr = sym.cbr_off.empty() ? 0 : sym.cbr_off.back();
+    d.sn_c0 = sn_c0.as<int>();
+    d.sn_f = sn_f.as<int>();
+    d.sn_rptr = sn_rptr.as<int>();
+    d.sn_rows = sn_rows.as<int>();
+    d.child_ptr = child_ptr.as<int>();
+    d.child_list = child_list.as<int>();
+    d.sn_parent = sn_parent.as<int>();
+    d.rel_ptr = rel_ptr.as<int>();
+    d.relmap = relmap.as<int>();
+    d.ah_ptr = ah_ptr.as<int>();
+    d.ah_loc = ah_loc.as<int>();
+    d.pan_off = pan_off.as<long long>();
+    d.cb_off = cb_off.as<long long>();
+    d.cbr_off = cbr_off.as<long long>();
+    return d;
+  }
+
+  void setup(const LUSymbolic& s, const std::vector<int>& ahp, const std::vector<int>& ahl, int nA_) {
+    sym = s;
+    nA = nA_;
+    upload(sn_c0, s.sn_c0);
+    upload(sn_f, s.sn_f);
+    upload(sn_rptr, s.sn_rptr);
+    upload(sn_rows, s.sn_rows);
+    upload(child_ptr, s.child_ptr);
+    upload(child_list, s.child_list);
+    upload(sn_parent, s.sn_parent);
+    upload(rel_ptr, s.rel_ptr);
+    upload(relmap, s.relmap);
+    upload(ah_ptr, ahp);
+    upload(ah_loc, ahl);
+    std::vector<long long> po(s.pan_off.begin(), s.pan_off.end()), co(s.cb_off.begin(), s.cb_off.end()),
+        ro(s.cbr_off.begin(), s.cbr_off.end());
+    upload(pan_off, po);
+    upload(cb_off, co);
+    upload(cbr_off, ro);
+    upload(lev_sn, s.lev_sn);
+    factor_sched.clear();
+    level_sched.clear();
+    for (int l = 0; l < s.nlevels; ++l) {
+      const int b = s.lev_ptr[l], e = s.lev_ptr[l + 1];
+      int fmax_all = 0;
+      for (int k = b; k < e; ++k) fmax_all = std::max(fmax_all, s.sn_f[s.lev_sn[k]]);
+      level_sched.push_back({b, e - b, 0, fmax_all});
+      int k = b;
+      while (k < e) {
+        const int f0 = s.sn_f[s.lev_sn[k]];
+        const int cls = f0 <= kFmaxS ? CLS_S : (f0 <= kFmaxM ? CLS_M : CLS_L);
+        int k2 = k, fcap = 0;
+        while (k2 < e) {
+          const int f = s.sn_f[s.lev_sn[k2]];
+          const int c2 = f <= kFmaxS ? CLS_S : (f <= kFmaxM ? CLS_M : CLS_L);
+          if (c2 != cls) break;
+          fcap = std::max(fcap, f);
+          ++k2;
+        }
+        factor_sched.push_back({k, k2 - k, cls, fcap});
+        k = k2;
+      }
+    }
+  }
+
+  void ensure_values(int prec, int ngroups) {
+    if (ngroups_alloc[prec] == ngroups && x[prec].p) return;
+    const size_t w = prec ? 4 : 8;
+    const size_t lanes = (size_t)ngroups * 32;
+    A[prec].alloc(lanes * w * (size_t)nA);
+    pan[prec].alloc(lanes * w * (size_t)sym.nnz);
+    cb[prec].alloc(lanes * w * (size_t)sym.sum_cb);
+    cbr[prec].alloc(lanes * w * (size_t)(sym.cbr_off.empty() ? 0 : sym.cbr_off.back()));
+    x[prec].alloc(lanes * w * (size_t)sym.n);
+    ngroups_alloc[prec] = ngroups;
+  }
+
+  void release_values() {
+    for (int p = 0; p < 2; ++p) {
+      A[p].release();
+      pan[p].release();
+      cb[p].release();
+      cbr[p].release();
+      x[p].release();
+      ngroups_alloc[p] = 0;
+    }
+  }
+};
+
+struct FDData {
+  DevBuf base, br_apos, br_bval;
+};
+
+// ------------------------------------------------------------------ kernel launchers
+template <typename T>
+struct Prec;
+template <>
+struct Prec<double> { static constexpr int idx = 0; static constexpr int G = 4; };
+template <>
+struct Prec<float> { static constexpr int idx = 1; static constexpr int G = 8; };
+
+template <typename T, int G, int TEAM>
+void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x,
+                       int* status, const int* group_active, int with_rhs, cudaStream_t st, int teams_per_block) {
+  const size_t team_elems = (size_t)ln.fcap * (ln.fcap + 1) * G;
+  const size_t smem = team_elems * sizeof(T) * teams_per_block;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, G, TEAM>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set = true;
+  }
+  const long long ntasks = (long long)ln.count * ngroups * (32 / G);
+  long long blocks = (ntasks + teams_per_block - 1) / teams_per_block;
+  blocks = std::min<long long>(blocks, 148LL * 32);
+  k_mf_factor<T, G, TEAM><<<(unsigned)blocks, TEAM * teams_per_block, smem, st>>>(
+      sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups, ln.fcap, A, pan, cb, cbr, x, status,
+      group_active, with_rhs);
+  CUDA_TRY(cudaGetLastError());
+}
+
+template <typename T>
+void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x, int* status,
+                   const int* group_active, int with_rhs, cudaStream_t st, int* nlaunch) {
+  constexpr int G = Prec<T>::G;
+  for (const Launch& ln : sys.factor_sched) {
+    if (ln.cls == CLS_S) {
+      // one case per thread, fronts up to 8 x 9
+      const int tpb = sizeof(T) == 8 ? 4 : 8;
+      launch_factor_one<T, 32, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, tpb);
+    } else if (ln.cls == CLS_M) {
+      launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 4);
+    } else {
+      launch_factor_one<T, G, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+    }
+    ++*nlaunch;
+  }
+}
+
+template <typename T>
+void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active, cudaStream_t st,
+                   int* nlaunch) {
+  for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
+    const Launch& ln = sys.level_sched[k];
+    const long long ntasks = (long long)ln.count * ngroups;
+    long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
+    k_mf_bsolve<T><<<(unsigned)blocks, 128, 0, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups,
+                                                     pan, x, group_active);
+    CUDA_TRY(cudaGetLastError());
+    ++*nlaunch;
+  }
+}
+
+template <typename T>
+void launch_fsolve(const LUSystem& sys, int ngroups, const T* pan, T* cbr, T* x, const int* group_active,
+                   cudaStream_t st, int* nlaunch) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_fsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set = true;
+  }
+  for (const Launch& ln : sys.level_sched) {
+    const long long ntasks = (long long)ln.count * ngroups;
+    long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
+    const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
+    k_mf_fsolve<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups,
+                                                        ln.fcap, pan, cbr, x, group_active);
+    CUDA_TRY(cudaGetLastError());
+    ++*nlaunch;
+  }
+}
+
+// ------------------------------------------------------------------ timing
+enum Family { FAM_MIS = 0, FAM_JAC, FAM_FACT, FAM_SOLVE, FAM_UPD, FAM_OTHER, FAM_N };
+
+struct EventTimer {
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::pair<int, int>> marks;  // (family, event index of start); end = start + 1
+  size_t used = 0;
+  cudaStream_t st = nullptr;
+  ~EventTimer() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+  void reset(cudaStream_t s) {
+    st = s;
+    used = 0;
+    marks.clear();
+  }
+  cudaEvent_t next() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      CUDA_TRY(cudaEventCreate(&e));
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  int begin(int fam) {
+    const int i = (int)used;
+    CUDA_TRY(cudaEventRecord(next(), st));
+    next();
+    marks.push_back({fam, i});
+    return i;
+  }
+  void end(int i) { CUDA_TRY(cudaEventRecord(pool[i + 1], st)); }
+  void collect(double* ms) {
+    for (int f = 0; f < FAM_N; ++f) ms[f] = 0.0;
+    for (auto& m : marks) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, pool[m.second], pool[m.second + 1]) == cudaSuccess) ms[m.first] += t;
+    }
+  }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------ handle
+struct mpf_handle {
+  std::string err;
+  mpf_options opt;
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  GridSymbolic g;
+  // shared device arrays
+  DevBuf y_rowptr, y_col, y_val, br_ypos, br_y, sbus0, v0, mis_rows, jvar, jpos;
+  LUSystem jac;
+  LUSystem bp[2], bpp[2];
+  FDData fdp[2], fdpp[2];
+  DevBuf fdvar;
+  bool fd_ready[2] = {false, false};
+  // cases
+  int ncases = 0, ngroups = 0, maxk = 0;
+  DevBuf out_br, sbus_case, V, Ibus, status, iters, maxmis, facc, group_active, any_active;
+  DevBuf vout, small_out;
+  bool have_cases = false, have_results = false;
+  int last_alg = -1, last_prec = -1;
+  cudaStream_t last_stream = nullptr;  // stream of the last solve / result copy
+  int* h_any = nullptr;  // pinned
+  EventTimer timer;
+  mpf_timing timing;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+
+  DevGrid dev() const {
+    DevGrid d;
+    d.nb = g.nb;
+    d.nfree = (int)g.mis_rows.size();
+    d.ngroups = ngroups;
+    d.n_jac = jac.sym.n;
+    d.nA_jac = jac.nA;
+    d.angle_mode = opt.angle_mode;
+    d.y_rowptr = y_rowptr.as<int>();
+    d.y_col = y_col.as<int>();
+    d.y_val = y_val.as<double2>();
+    d.br_ypos = br_ypos.as<int4>();
+    d.br_y = br_y.as<double2>();
+    d.sbus0 = sbus0.as<double2>();
+    d.sbus_case = sbus_case.p ? sbus_case.as<double2>() : nullptr;
+    d.v0 = v0.as<double2>();
+    d.mis_rows = mis_rows.as<int>();
+    d.jvar = jvar.as<int2>();
+    d.jpos = jpos.as<int4>();
+    d.out_br = out_br.as<int>();
+    d.V = V.as<double2>();
+    d.Ibus = Ibus.as<double2>();
+    d.status = status.as<int>();
+    d.iters = iters.as<int>();
+    d.maxmis = maxmis.as<double>();
+    d.facc = facc.as<unsigned long long>();
+    d.group_active = group_active.as<int>();
+    d.any_active = any_active.as<int>();
+    return d;
+  }
+
+  size_t device_bytes() const {
+    size_t b = 0;
+    const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
+                           &out_br, &sbus_case, &V, &Ibus, &status, &iters, &maxmis, &facc, &group_active,
+                           &any_active, &vout, &small_out, &fdvar};
+    for (auto p : all) b += p->bytes;
+    const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
+    for (auto s : systems) {
+      for (int p = 0; p < 2; ++p) b += s->A[p].bytes + s->pan[p].bytes + s->cb[p].bytes + s->cbr[p].bytes + s->x[p].bytes;
+      const DevBuf* idx[] = {&s->sn_c0, &s->sn_f, &s->sn_rptr, &s->sn_rows, &s->child_ptr, &s->child_list,
+                             &s->sn_parent, &s->rel_ptr, &s->relmap, &s->ah_ptr, &s->ah_loc, &s->pan_off,
+                             &s->cb_off, &s->cbr_off, &s->lev_sn};
+      for (auto q : idx) b += q->bytes;
+    }
+    for (int v = 0; v < 2; ++v) b += fdp[v].base.bytes + fdp[v].br_apos.bytes + fdp[v].br_bval.bytes +
+                                     fdpp[v].base.bytes + fdpp[v].br_apos.bytes + fdpp[v].br_bval.bytes;
+    return b;
+  }
+};
+
+namespace {
+
+int fail(mpf_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+template <class F>
+int guarded(mpf_handle* h, F&& f) {
+  try {
+    return f();
+  } catch (const MpfError& e) {
+    return fail(h, e.code, e.msg);
+  } catch (const std::bad_alloc&) {
+    return fail(h, MPF_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(h, MPF_ERR_INTERNAL, e.what());
+  }
+}
+
+void upload_fd(mpf_handle* h, int variant) {
+  if (h->fd_ready[variant]) return;
+  const GridSymbolic& g = h->g;
+  auto setup_one = [&](const GridSymbolic::FDSystem& fs, LUSystem& sys, FDData& fd) {
+    sys.setup(fs.lu, fs.ah_ptr, fs.ah_loc, (int)fs.base.size());
+    upload(fd.base, fs.base);
+    std::vector<int4> pos(g.nbr);
+    std::vector<double4> val(g.nbr);
+    for (int e = 0; e < g.nbr; ++e) {
+      pos[e] = make_int4(fs.br_pos[4 * e], fs.br_pos[4 * e + 1], fs.br_pos[4 * e + 2], fs.br_pos[4 * e + 3]);
+      val[e] = make_double4(fs.br_val[4 * e], fs.br_val[4 * e + 1], fs.br_val[4 * e + 2], fs.br_val[4 * e + 3]);
+    }
+    upload(fd.br_apos, pos);
+    upload(fd.br_bval, val);
+  };
+  setup_one(g.bp[variant], h->bp[variant], h->fdp[variant]);
+  setup_one(g.bpp[variant], h->bpp[variant], h->fdpp[variant]);
+  if (!h->fdvar.p) {
+    std::vector<int2> fv(g.nb);
+    for (int i = 0; i < g.nb; ++i) fv[i] = make_int2(g.bp[0].var[i], g.bpp[0].var[i]);
+    upload(h->fdvar, fv);
+  }
+  h->fd_ready[variant] = true;
+}
+
+dim3 row_grid(const mpf_handle* h) {
+  const int nfree = (int)h->g.mis_rows.size();
+  return dim3((unsigned)((nfree + kRowsPerBlock - 1) / kRowsPerBlock), (unsigned)h->ngroups);
+}
+
+bool any_active(mpf_handle* h, cudaStream_t st) {
+  CUDA_TRY(cudaMemcpyAsync(h->h_any, h->any_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return *h->h_any != 0;
+}
+
+void check(mpf_handle* h, cudaStream_t st, int it, int max_it, int* nl) {
+  CUDA_TRY(cudaMemsetAsync(h->any_active.p, 0, sizeof(int), st));
+  const int nl_lanes = h->ngroups * 32;
+  k_check<<<(nl_lanes + 255) / 256, 256, 0, st>>>(h->dev(), it, max_it, h->opt.tol);
+  CUDA_TRY(cudaGetLastError());
+  ++*nl;
+}
+
+template <typename T>
+void solve_nr(mpf_handle* h, cudaStream_t st) {
+  constexpr int P = Prec<T>::idx;
+  LUSystem& J = h->jac;
+  J.ensure_values(P, h->ngroups);
+  T* A = J.A[P].as<T>();
+  T* pan = J.pan[P].as<T>();
+  T* cb = J.cb[P].as<T>();
+  T* cbr = J.cbr[P].as<T>();
+  T* x = J.x[P].as<T>();
+  const DevGrid d = h->dev();
+  const dim3 rg = row_grid(h);
+  int nl = 0;
+  EventTimer& tm = h->timer;
+  int ev = tm.begin(FAM_OTHER);
+  k_init<<<std::min(148 * 8, (int)((size_t)h->ngroups * h->g.nb * 32 / 256 + 1)), 256, 0, st>>>(d, h->ncases);
+  CUDA_TRY(cudaGetLastError());
+  ++nl;
+  tm.end(ev);
+  const int max_it = h->opt.max_it_nr;
+  int it = 0;
+  for (;; ++it) {
+    ev = tm.begin(FAM_MIS);
+    k_mismatch_nr<T><<<rg, 256, 0, st>>>(d, x);
+    CUDA_TRY(cudaGetLastError());
+    ++nl;
+    tm.end(ev);
+    ev = tm.begin(FAM_OTHER);
+    check(h, st, it, max_it, &nl);
+    tm.end(ev);
+    if (it >= max_it || !any_active(h, st)) break;
+    ev = tm.begin(FAM_JAC);
+    k_jfill<T><<<rg, 256, 0, st>>>(d, A);
+    CUDA_TRY(cudaGetLastError());
+    ++nl;
+    tm.end(ev);
+    ev = tm.begin(FAM_FACT);
+    launch_factor<T>(J, h->ngroups, A, pan, cb, cbr, x, d.status, d.group_active, 1, st, &nl);
+    tm.end(ev);
+    ev = tm.begin(FAM_SOLVE);
+    launch_bsolve<T>(J, h->ngroups, pan, x, d.group_active, st, &nl);
+    tm.end(ev);
+    ev = tm.begin(FAM_UPD);
+    k_update_nr<T><<<rg, 256, 0, st>>>(d, x);
+    CUDA_TRY(cudaGetLastError());
+    ++nl;
+    tm.end(ev);
+  }
+  h->timing.launches = nl;
+  h->timing.iterations_max = it;
+}
+
+template <typename T>
+void solve_fd(mpf_handle* h, cudaStream_t st, int variant) {
+  constexpr int P = Prec<T>::idx;
+  upload_fd(h, variant);
+  LUSystem& Bp = h->bp[variant];
+  LUSystem& Bpp = h->bpp[variant];
+  Bp.ensure_values(P, h->ngroups);
+  Bpp.ensure_values(P, h->ngroups);
+  const DevGrid d = h->dev();
+  DevFD fdd;
+  fdd.n_bp = Bp.sym.n;
+  fdd.n_bpp = Bpp.sym.n;
+  fdd.fdvar = h->fdvar.as<int2>();
+  const dim3 rg = row_grid(h);
+  int nl = 0;
+  EventTimer& tm = h->timer;
+  int ev = tm.begin(FAM_OTHER);
+  k_init<<<std::min(148 * 8, (int)((size_t)h->ngroups * h->g.nb * 32 / 256 + 1)), 256, 0, st>>>(d, h->ncases);
+  CUDA_TRY(cudaGetLastError());
+  ++nl;
+  tm.end(ev);
+  // B' and B'' of every case, factorised once and reused by all iterations
+  ev = tm.begin(FAM_JAC);
+  LUSystem* systems[2] = {&Bp, &Bpp};
+  FDData* fds[2] = {&h->fdp[variant], &h->fdpp[variant]};
+  for (int k = 0; k < 2; ++k) {
+    LUSystem& S = *systems[k];
+    const size_t total = (size_t)h->ngroups * S.nA * 32;
+    k_fd_base<T><<<(unsigned)std::min<size_t>(148 * 16, total / 256 + 1), 256, 0, st>>>(
+        h->ngroups, S.nA, fds[k]->base.as<double>(), S.A[P].as<T>());
+    CUDA_TRY(cudaGetLastError());
+    k_fd_outage<T><<<(h->ngroups * 32 + 127) / 128, 128, 0, st>>>(d, S.nA, fds[k]->br_apos.as<int4>(),
+                                                                    fds[k]->br_bval.as<double4>(), S.A[P].as<T>());
+    CUDA_TRY(cudaGetLastError());
+    nl += 2;
+  }
+  tm.end(ev);
+  ev = tm.begin(FAM_FACT);
+  for (int k = 0; k < 2; ++k) {
+    LUSystem& S = *systems[k];
+    launch_factor<T>(S, h->ngroups, S.A[P].as<T>(), S.pan[P].as<T>(), S.cb[P].as<T>(), S.cbr[P].as<T>(),
+                     S.x[P].as<T>(), d.status, d.group_active, 0, st, &nl);
+  }
+  tm.end(ev);
+  T* xp = Bp.x[P].as<T>();
+  T* xq = Bpp.x[P].as<T>();
+  const int max_it = h->opt.max_it_fd;
+  auto mismatch = [&]() {
+    int e2 = tm.begin(FAM_MIS);
+    k_mismatch_fd<T><<<rg, 256, 0, st>>>(d, fdd, xp, xq);
+    CUDA_TRY(cudaGetLastError());
+    ++nl;
+    tm.end(e2);
+  };
+  mismatch();
+  ev = tm.begin(FAM_OTHER);
+  check(h, st, 0, max_it, &nl);
+  tm.end(ev);
+  int i = 0;
+  if (any_active(h, st)) {
+    while (i < max_it) {
+      ++i;
+      for (int half = 0; half < 2; ++half) {
+        LUSystem& S = half == 0 ? Bp : Bpp;
+        ev = tm.begin(FAM_SOLVE);
+        launch_fsolve<T>(S, h->ngroups, S.pan[P].as<T>(), S.cbr[P].as<T>(), S.x[P].as<T>(), d.group_active, st, &nl);
+        launch_bsolve<T>(S, h->ngroups, S.pan[P].as<T>(), S.x[P].as<T>(), d.group_active, st, &nl);
+        tm.end(ev);
+        ev = tm.begin(FAM_UPD);
+        k_update_fd<T><<<rg, 256, 0, st>>>(d, fdd, xp, xq, half);
+        CUDA_TRY(cudaGetLastError());
+        ++nl;
+        tm.end(ev);
+        mismatch();
+        ev = tm.begin(FAM_OTHER);
+        // after the P half only convergence retires a case (fdpf.h:529-540); the
+        // iteration limit is tested after the Q half
+        check(h, st, i, half == 0 ? INT32_MAX : max_it, &nl);
+        tm.end(ev);
+        if (!any_active(h, st)) break;
+      }
+      if (*h->h_any == 0) break;
+    }
+  }
+  h->timing.launches = nl;
+  h->timing.iterations_max = i;
+}
+
+}  // namespace
+
+// ====================================================================== C-ABI
+extern "C" {
+
+int32_t mpf_abi_version(void) { return MPF_ABI_VERSION; }
+
+void mpf_default_options(mpf_options* opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->max_it_nr = MPF_DEFAULT_MAX_IT_NR;
+  opt->max_it_fd = MPF_DEFAULT_MAX_IT_FD;
+  opt->tol = MPF_DEFAULT_TOL;
+  opt->angle_mode = 0;
+  opt->device = 0;
+  opt->use_graph = 1;
+}
+
+const char* mpf_status_string(int32_t status) {
+  switch (status) {
+    case MPF_OK: return "ok";
+    case MPF_ERR_BAD_INPUT: return "bad input";
+    case MPF_ERR_CUDA: return "CUDA error";
+    case MPF_ERR_OOM: return "out of memory";
+    case MPF_ERR_STATE: return "call out of order";
+    case MPF_ERR_TIMEOUT: return "device wait timed out";
+    case MPF_ERR_INTERNAL: return "internal error";
+    case MPF_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* mpf_last_error(const mpf_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branches, int32_t n_branch,
+                   const mpf_options* opt, mpf_handle** out) {
+  if (!out) return MPF_ERR_BAD_INPUT;
+  *out = nullptr;
+  if (!buses || !branches || n_bus < 2 || n_branch < 1) return MPF_ERR_BAD_INPUT;
+  std::unique_ptr<mpf_handle> h(new (std::nothrow) mpf_handle());
+  if (!h) return MPF_ERR_OOM;
+  mpf_default_options(&h->opt);
+  if (opt) h->opt = *opt;
+  if (h->opt.max_it_nr < 0 || h->opt.max_it_fd < 0 || !(h->opt.tol > 0.0) ||
+      (h->opt.angle_mode != 0 && h->opt.angle_mode != 1)) {
+    h->err = "invalid options";
+    *out = h.release();
+    return MPF_ERR_BAD_INPUT;
+  }
+  int rc = guarded(h.get(), [&]() -> int {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(h.get(), MPF_ERR_NO_DEVICE, "no CUDA device visible");
+    if (h->opt.device < 0 || h->opt.device >= ndev) return fail(h.get(), MPF_ERR_BAD_INPUT, "device ordinal out of range");
+    h->device = h->opt.device;
+    CUDA_TRY(cudaSetDevice(h->device));
+    const std::string msg = build_symbolic(buses, n_bus, branches, n_branch, h->g);
+    if (!msg.empty()) return fail(h.get(), MPF_ERR_BAD_INPUT, msg);
+    const GridSymbolic& g = h->g;
+    int maxf = g.jac.max_front;
+    for (int v = 0; v < 2; ++v) maxf = std::max({maxf, g.bp[v].lu.max_front, g.bpp[v].lu.max_front});
+    if (maxf > kFmaxL)
+      return fail(h.get(), MPF_ERR_BAD_INPUT,
+                  "largest frontal matrix (" + std::to_string(maxf) + ") exceeds the supported " +
+                      std::to_string(kFmaxL) + " (grid too densely meshed for shared-memory fronts)");
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaMallocHost(&h->h_any, sizeof(int)));
+    CUDA_TRY(cudaEventCreate(&h->t0));
+    CUDA_TRY(cudaEventCreate(&h->t1));
+    upload(h->y_rowptr, g.y_rowptr);
+    upload(h->y_col, g.y_col);
+    {
+      std::vector<double2> yv(g.y_val.size() / 2);
+      for (size_t k = 0; k < yv.size(); ++k) yv[k] = make_double2(g.y_val[2 * k], g.y_val[2 * k + 1]);
+      upload(h->y_val, yv);
+      std::vector<int4> bp(g.nbr);
+      std::vector<double2> by(4 * (size_t)g.nbr);
+      for (int e = 0; e < g.nbr; ++e) {
+        bp[e] = make_int4(g.br_pos[4 * e], g.br_pos[4 * e + 1], g.br_pos[4 * e + 2], g.br_pos[4 * e + 3]);
+        for (int q = 0; q < 4; ++q) by[4 * e + q] = make_double2(g.br_y[8 * e + 2 * q], g.br_y[8 * e + 2 * q + 1]);
+      }
+      upload(h->br_ypos, bp);
+      upload(h->br_y, by);
+      std::vector<double2> sb(g.nb), v0(g.nb);
+      for (int i = 0; i < g.nb; ++i) {
+        sb[i] = make_double2(g.sbus[2 * i], g.sbus[2 * i + 1]);
+        v0[i] = make_double2(g.v0[2 * i], g.v0[2 * i + 1]);
+      }
+      upload(h->sbus0, sb);
+      upload(h->v0, v0);
+      upload(h->mis_rows, g.mis_rows);
+      std::vector<int2> jv(g.nb);
+      for (int i = 0; i < g.nb; ++i) jv[i] = make_int2(g.var_va[i], g.var_vm[i]);
+      upload(h->jvar, jv);
+      std::vector<int4> jp(g.y_col.size());
+      for (size_t p = 0; p < jp.size(); ++p)
+        jp[p] = make_int4(g.jpos[4 * p], g.jpos[4 * p + 1], g.jpos[4 * p + 2], g.jpos[4 * p + 3]);
+      upload(h->jpos, jp);
+    }
+    h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac);
+    h->any_active.alloc(sizeof(int));
+    return MPF_OK;
+  });
+  *out = h.release();
+  return rc;
+}
+
+int32_t mpf_destroy(mpf_handle* h) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (h->own_stream) {
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->own_stream);
+    cudaStreamDestroy(h->own_stream);
+  }
+  if (h->h_any) cudaFreeHost(h->h_any);
+  if (h->t0) cudaEventDestroy(h->t0);
+  if (h->t1) cudaEventDestroy(h->t1);
+  delete h;
+  return MPF_OK;
+}
+
+int32_t mpf_get_stats(const mpf_handle* h, mpf_stats* st) {
+  if (!h || !st) return MPF_ERR_BAD_INPUT;
+  std::memset(st, 0, sizeof(*st));
+  const GridSymbolic& g = h->g;
+  st->n_bus = g.nb;
+  st->n_branch = g.nbr;
+  st->n_pv = g.npv;
+  st->n_pq = g.npq;
+  st->n_slack = g.slack >= 0 ? 1 : 0;
+  st->nnz_ybus = g.y_rowptr.empty() ? 0 : g.y_rowptr.back();
+  st->n_jac = g.jac.n;
+  st->nnz_jac = g.nnz_jac;
+  st->nnz_lu = (int32_t)g.jac.nnz;
+  st->lu_levels = g.jac.nlevels;
+  st->lu_flops = g.jac.flops;
+  st->n_bp = g.bp[0].lu.n;
+  st->nnz_bp_lu = (int32_t)g.bp[0].lu.nnz;
+  st->bp_levels = g.bp[0].lu.nlevels;
+  st->n_bpp = g.bpp[0].lu.n;
+  st->nnz_bpp_lu = (int32_t)g.bpp[0].lu.nnz;
+  st->bpp_levels = g.bpp[0].lu.nlevels;
+  st->n_cases = h->ncases;
+  st->case_groups = h->ngroups;
+  st->device_bytes = (int64_t)h->device_bytes();
+  return MPF_OK;
+}
+
+int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases, const int32_t* outage_offsets, const int32_t* outage_branches,
+                      const double* sbus) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (n_cases < 1) return fail(h, MPF_ERR_BAD_INPUT, "n_cases must be >= 1");
+  if ((outage_offsets == nullptr) != (outage_branches == nullptr) && outage_offsets && outage_offsets[n_cases] > 0)
+    return fail(h, MPF_ERR_BAD_INPUT, "outage_offsets given without outage_branches");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    // the case buffers are rewritten below: wait for work that may still read them
+    CUDA_TRY(cudaStreamSynchronize(h->own_stream));
+    if (h->last_stream) CUDA_TRY(cudaStreamSynchronize(h->last_stream));
+    const GridSymbolic& g = h->g;
+    const int ngroups = (n_cases + 31) / 32;
+    const int lanes = ngroups * 32;
+    std::vector<int> outs((size_t)kMaxOut * lanes, -1);
+    int maxk = 0;
+    if (outage_offsets) {
+      if (outage_offsets[0] != 0) return fail(h, MPF_ERR_BAD_INPUT, "outage_offsets[0] must be 0");
+      for (int c = 0; c < n_cases; ++c) {
+        const int b = outage_offsets[c], e = outage_offsets[c + 1];
+        if (e < b) return fail(h, MPF_ERR_BAD_INPUT, "outage_offsets must be non-decreasing");
+        if (e - b > kMaxOut)
+          return fail(h, MPF_ERR_BAD_INPUT, "case " + std::to_string(c) + " outages more than " +
+                                                std::to_string(kMaxOut) + " branches");
+        for (int k = b; k < e; ++k) {
+          const int br = outage_branches[k];
+          if (br < 0 || br >= g.nbr)
+            return fail(h, MPF_ERR_BAD_INPUT, "case " + std::to_string(c) + ": outaged branch index out of range");
+          for (int k2 = b; k2 < k; ++k2)
+            if (outage_branches[k2] == br)
+              return fail(h, MPF_ERR_BAD_INPUT, "case " + std::to_string(c) + " lists a branch twice");
+          outs[(size_t)(k - b) * lanes + c] = br;
+        }
+        maxk = std::max(maxk, e - b);
+      }
+    }
+    std::vector<double2> sb;
+    if (sbus) {
+      sb.assign((size_t)ngroups * g.nb * 32, make_double2(0.0, 0.0));
+      for (int c = 0; c < n_cases; ++c)
+        for (int i = 0; i < g.nb; ++i) {
+          const double p = sbus[((size_t)c * g.nb + i) * 2], q = sbus[((size_t)c * g.nb + i) * 2 + 1];
+          if (!std::isfinite(p) || !std::isfinite(q))
+            return fail(h, MPF_ERR_BAD_INPUT, "sbus has a non-finite value");
+          sb[((size_t)(c >> 5) * g.nb + i) * 32 + (c & 31)] = make_double2(p, q);
+        }
+    }
+    if (ngroups != h->ngroups) {
+      const size_t per_bus = (size_t)ngroups * g.nb * 32 * sizeof(double2);
+      h->V.alloc(per_bus);
+      h->Ibus.alloc(per_bus);
+      h->status.alloc(lanes * sizeof(int));
+      h->iters.alloc(lanes * sizeof(int));
+      h->maxmis.alloc(lanes * sizeof(double));
+      h->facc.alloc(lanes * sizeof(unsigned long long));
+      h->group_active.alloc(ngroups * sizeof(int));
+      h->vout.release();
+      h->small_out.release();
+      h->jac.release_values();
+      for (int v = 0; v < 2; ++v) {
+        h->bp[v].release_values();
+        h->bpp[v].release_values();
+      }
+    }
+    upload(h->out_br, outs);
+    if (sbus) upload(h->sbus_case, sb);
+    else h->sbus_case.release();
+    h->ncases = n_cases;
+    h->ngroups = ngroups;
+    h->maxk = maxk;
+    h->have_cases = true;
+    h->have_results = false;
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_solve(mpf_handle* h, int32_t alg, int32_t precision, void* stream) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (!h->have_cases) return fail(h, MPF_ERR_STATE, "mpf_set_cases must be called before mpf_solve");
+  if (alg != MPF_NR && alg != MPF_FDXB && alg != MPF_FDBX) return fail(h, MPF_ERR_BAD_INPUT, "unknown algorithm");
+  if (precision != MPF_FP64 && precision != MPF_MIXED) return fail(h, MPF_ERR_BAD_INPUT, "unknown precision");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->own_stream;
+    h->last_stream = st;
+    std::memset(&h->timing, 0, sizeof(h->timing));
+    h->timer.reset(st);
+    CUDA_TRY(cudaEventRecord(h->t0, st));
+    if (alg == MPF_NR) {
+      if (precision == MPF_FP64) solve_nr<double>(h, st);
+      else solve_nr<float>(h, st);
+    } else {
+      const int variant = alg == MPF_FDXB ? 0 : 1;
+      if (precision == MPF_FP64) solve_fd<double>(h, st, variant);
+      else solve_fd<float>(h, st, variant);
+    }
+    CUDA_TRY(cudaEventRecord(h->t1, st));
+    CUDA_TRY(cudaGetLastError());
+    h->have_results = true;
+    h->last_alg = alg;
+    h->last_prec = precision;
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_get_timing(mpf_handle* h, mpf_timing* t) {
+  if (!h || !t) return MPF_ERR_BAD_INPUT;
+  if (!h->have_results) return fail(h, MPF_ERR_STATE, "no solve to report");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaEventSynchronize(h->t1));
+    double ms[FAM_N];
+    h->timer.collect(ms);
+    float tot = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&tot, h->t0, h->t1));
+    h->timing.total_ms = tot;
+    h->timing.mismatch_ms = ms[FAM_MIS];
+    h->timing.jacobian_ms = ms[FAM_JAC];
+    h->timing.factor_ms = ms[FAM_FACT];
+    h->timing.solve_ms = ms[FAM_SOLVE];
+    h->timing.update_ms = ms[FAM_UPD];
+    h->timing.other_ms = ms[FAM_OTHER];
+    *t = h->timing;
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_get_results_device(mpf_handle* h, double* v, int32_t* iterations, uint8_t* status, double* max_mis,
+                               void* stream) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (!h->have_results) return fail(h, MPF_ERR_STATE, "no results: call mpf_solve first");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->own_stream;
+    if (v) {
+      const size_t total = (size_t)h->ncases * h->g.nb;
+      k_gather_v<<<(unsigned)std::min<size_t>(148 * 16, total / 256 + 1), 256, 0, st>>>(
+          h->g.nb, h->ncases, h->V.as<double2>(), reinterpret_cast<double2*>(v));
+      CUDA_TRY(cudaGetLastError());
+    }
+    if (iterations || status || max_mis) {
+      k_gather_small<<<(h->ncases + 255) / 256, 256, 0, st>>>(h->ncases, h->status.as<int>(), h->iters.as<int>(),
+                                                             h->maxmis.as<double>(), status, iterations, max_mis);
+      CUDA_TRY(cudaGetLastError());
+    }
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_get_results(mpf_handle* h, double* v, int32_t* iterations, uint8_t* status, double* max_mis) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (!h->have_results) return fail(h, MPF_ERR_STATE, "no results: call mpf_solve first");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st = h->own_stream;
+    const size_t vbytes = (size_t)h->ncases * h->g.nb * sizeof(double2);
+    const size_t sbytes = (size_t)h->ncases * (sizeof(int) + sizeof(double) + 1) + 64;
+    if (h->vout.bytes < vbytes) h->vout.alloc(vbytes);
+    if (h->small_out.bytes < sbytes) h->small_out.alloc(sbytes);
+    int32_t* d_it = h->small_out.as<int32_t>();
+    double* d_mm = reinterpret_cast<double*>(reinterpret_cast<char*>(h->small_out.p) + ((h->ncases * sizeof(int) + 15) / 16) * 16);
+    uint8_t* d_st = reinterpret_cast<uint8_t*>(d_mm + h->ncases);
+    // the solve may have run on a caller stream: order after it
+    CUDA_TRY(cudaStreamWaitEvent(st, h->t1, 0));
+    int rc = mpf_get_results_device(h, v ? h->vout.as<double>() : nullptr, d_it, d_st, d_mm, st);
+    if (rc != MPF_OK) return rc;
+    if (v) CUDA_TRY(cudaMemcpyAsync(v, h->vout.p, vbytes, cudaMemcpyDeviceToHost, st));
+    if (iterations) CUDA_TRY(cudaMemcpyAsync(iterations, d_it, h->ncases * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    if (max_mis) CUDA_TRY(cudaMemcpyAsync(max_mis, d_mm, h->ncases * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (status) CUDA_TRY(cudaMemcpyAsync(status, d_st, h->ncases, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_runpf_host(mpf_handle* h, int32_t alg, int32_t precision, int32_t n_cases, const int32_t* outage_offsets,
+                       const int32_t* outage_branches, const double* sbus, double* v, int32_t* iterations,
+                       uint8_t* status, double* max_mis) {
+  int rc = mpf_set_cases(h, n_cases, outage_offsets, outage_branches, sbus);
+  if (rc != MPF_OK) return rc;
+  rc = mpf_solve(h, alg, precision, nullptr);
+  if (rc != MPF_OK) return rc;
+  return mpf_get_results(h, v, iterations, status, max_mis);
+}
+
+}  // extern "C"

@@ -1,0 +1,574 @@
+// Device kernels of the batched power flow (sm_100a).
+//
+// Batch layout: cases are lanes.  Every per-case array is stored as
+// [group][entry][32]: case c lives in group c / 32, lane c % 32, so a warp that
+// handles one entry (a bus, a Jacobian entry, a factor entry) for the 32 cases of a
+// group reads or writes one contiguous 256-byte (FP64) or 128-byte (FP32) row.
+// Index arrays (Ybus pattern, front structures) are shared by all lanes.
+//
+// Per Newton iteration (newtonpf.h:365-523 does the same steps for one case):
+//   k_mismatch_nr   Ibus = Ybus V, mis = V conj(Ibus) - Sbus, F into the LU
+//                   right-hand side, per-case max |F|       (newtonpf.h:18-95)
+//   k_check         per-case convergence / iteration-limit / divergence mask
+//   k_jfill         Jacobian entries straight into the factor input (A-array)
+//                                                           (newtonpf.h:97-186)
+//   k_mf_factor     multifrontal LU of all cases, level by level, forward
+//                   substitution of F carried through the fronts
+//   k_mf_bsolve     backward substitution, level by level (top down)
+//   k_update_nr     polar voltage update V <- (|V| - dVm) e^{j(Va - dVa)}
+//                                                           (newtonpf.h:188-213)
+// Each case's Ybus is the superset base minus its outaged branches, applied on the
+// fly where an entry is read (no per-case Ybus, no SpGEMM).
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace mpfk {
+
+constexpr int kMaxOut = 4;  // outaged branches per case
+
+enum : int { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAX_ITER = 2, ST_DIVERGED = 3, ST_SINGULAR = 4 };
+
+__device__ __forceinline__ size_t at32(int g, long long n, long long e, int lane) {
+  return ((size_t)g * (size_t)n + (size_t)e) * 32 + lane;
+}
+
+struct DevGrid {
+  int nb, nfree, ngroups, n_jac, nA_jac;
+  int angle_mode;
+  const int* y_rowptr;
+  const int* y_col;
+  const double2* y_val;
+  const int4* br_ypos;      // per branch: Ybus positions (ff, ft, tf, tt)
+  const double2* br_y;      // per branch: 4 admittances
+  const double2* sbus0;     // [nb]
+  const double2* sbus_case; // [g][nb][32] or null
+  const double2* v0;        // [nb]
+  const int* mis_rows;      // [nfree] PV/PQ buses
+  const int2* jvar;         // [nb] (Va var, Vm var) of the Newton system, -1 if none
+  const int4* jpos;         // [nnzY] A-array index of the 4 Jacobian quadrants, -1 if none
+  const int* out_br;        // [kMaxOut][ngroups*32] outaged branch or -1
+  double2* V;               // [g][nb][32]
+  double2* Ibus;            // [g][nb][32]
+  int* status;              // [ngroups*32]
+  int* iters;
+  double* maxmis;
+  unsigned long long* facc; // running max |F| (bits of a non-negative double)
+  int* group_active;        // [ngroups]
+  int* any_active;          // [1]
+};
+
+struct DevLU {
+  int n, nsn, nA;
+  long long nnz, sumcb, sumcbr;
+  const int* sn_c0;
+  const int* sn_f;
+  const int* sn_rptr;
+  const int* sn_rows;
+  const int* child_ptr;
+  const int* child_list;
+  const int* sn_parent;
+  const int* rel_ptr;
+  const int* relmap;
+  const int* ah_ptr;
+  const int* ah_loc;
+  const long long* pan_off;
+  const long long* cb_off;
+  const long long* cbr_off;
+};
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+struct LaneOut {
+  int e[kMaxOut];
+  int4 pos[kMaxOut];
+};
+
+__device__ __forceinline__ void load_outages(const DevGrid& d, int c, LaneOut& o) {
+  const int stride = d.ngroups * 32;
+#pragma unroll
+  for (int k = 0; k < kMaxOut; ++k) {
+    o.e[k] = d.out_br[k * stride + c];
+    o.pos[k] = o.e[k] >= 0 ? d.br_ypos[o.e[k]] : make_int4(-1, -1, -1, -1);
+  }
+}
+
+// Ybus entry p of this case: base value minus the outaged branches' parts
+// (makeYbus.h:69-73 scales a branch by its status; status 0 removes it).
+__device__ __forceinline__ double2 ycase(const DevGrid& d, const LaneOut& o, int p, double2 y) {
+#pragma unroll
+  for (int k = 0; k < kMaxOut; ++k) {
+    if (o.e[k] < 0) continue;
+    const int4 q = o.pos[k];
+    const double2* by = d.br_y + 4 * o.e[k];
+    if (p == q.x) { const double2 t = by[0]; y.x -= t.x; y.y -= t.y; }
+    if (p == q.y) { const double2 t = by[1]; y.x -= t.x; y.y -= t.y; }
+    if (p == q.z) { const double2 t = by[2]; y.x -= t.x; y.y -= t.y; }
+    if (p == q.w) { const double2 t = by[3]; y.x -= t.x; y.y -= t.y; }
+  }
+  return y;
+}
+
+__device__ __forceinline__ double vangle(double2 v, int mode) {
+  return mode == 1 ? atan(v.y / v.x) : atan2(v.y, v.x);
+}
+
+__device__ __forceinline__ double finite_or_inf(double m) { return (m <= DBL_MAX) ? m : INFINITY; }
+
+// block-wide per-lane max of 8 warps, then one atomicMax per lane
+__device__ __forceinline__ void block_lane_max(double v, unsigned long long* dst, bool active) {
+  __shared__ double red[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  red[warp][lane] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double m = red[0][lane];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) m = fmax(m, red[k][lane]);
+    if (active) atomicMax(dst, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// ---------------------------------------------------------------- init / check
+__global__ void k_init(DevGrid d, int ncases) {
+  const size_t total = (size_t)d.ngroups * d.nb * 32;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)((t >> 5) % d.nb);
+    d.V[t] = d.v0[i];
+  }
+  const int nl = d.ngroups * 32;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nl; c += gridDim.x * blockDim.x) {
+    d.status[c] = c < ncases ? ST_RUNNING : ST_CONVERGED;
+    d.iters[c] = 0;
+    d.maxmis[c] = 0.0;
+    d.facc[c] = 0ull;
+  }
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < d.ngroups; g += gridDim.x * blockDim.x)
+    d.group_active[g] = 1;
+}
+
+// One thread per case (a warp = a group): decide convergence of the mismatch just
+// evaluated.  it = iterations done so far; the reference loop stops when
+// max |F| < tol or it == max_it (newtonpf.h:394-398, 518).
+__global__ void k_check(DevGrid d, int it, int max_it, double tol) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nl = d.ngroups * 32;
+  bool active = false;
+  if (c < nl) {
+    if (d.status[c] == ST_RUNNING) {
+      const double m = __longlong_as_double((long long)d.facc[c]);
+      d.maxmis[c] = m;
+      d.iters[c] = it;
+      if (!(m <= DBL_MAX)) d.status[c] = ST_DIVERGED;
+      else if (m < tol) d.status[c] = ST_CONVERGED;
+      else if (it >= max_it) d.status[c] = ST_MAX_ITER;
+      else active = true;
+    }
+    d.facc[c] = 0ull;
+  }
+  const unsigned any = __ballot_sync(0xffffffffu, active);
+  if ((threadIdx.x & 31) == 0 && c < nl) {
+    d.group_active[c >> 5] = any != 0u;
+    if (any) atomicAdd(d.any_active, 1);
+  }
+}
+
+// ---------------------------------------------------------------- Newton mismatch
+// grid (row blocks, groups); 8 warps per block; a warp = one bus row x 32 cases.
+constexpr int kRowsPerBlock = 64;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x) {
+  const int g = blockIdx.y;
+  if (!d.group_active[g]) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = g * 32 + lane;
+  LaneOut o;
+  load_outages(d, c, o);
+  double lmax = 0.0;
+  const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
+  for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
+    const int i = d.mis_rows[r];
+    double2 ib = make_double2(0.0, 0.0);
+    for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
+      const double2 y = ycase(d, o, p, d.y_val[p]);
+      const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
+      ib.x += y.x * v.x - y.y * v.y;
+      ib.y += y.x * v.y + y.y * v.x;
+    }
+    const double2 vi = d.V[at32(g, d.nb, i, lane)];
+    const double2 s = d.sbus_case ? d.sbus_case[at32(g, d.nb, i, lane)] : d.sbus0[i];
+    // mis = V conj(Ibus) - S
+    const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
+    const double mi = vi.y * ib.x - vi.x * ib.y - s.y;
+    d.Ibus[at32(g, d.nb, i, lane)] = ib;
+    const int2 jv = d.jvar[i];
+    x[at32(g, d.n_jac, jv.x, lane)] = (T)mr;
+    double m = fabs(mr);
+    if (jv.y >= 0) {
+      x[at32(g, d.n_jac, jv.y, lane)] = (T)mi;
+      m = fmax(m, fabs(mi));
+      if (mi != mi) m = INFINITY;
+    }
+    if (mr != mr) m = INFINITY;
+    lmax = fmax(lmax, finite_or_inf(m));
+  }
+  block_lane_max(lmax, &d.facc[c], d.status[c] == ST_RUNNING);
+}
+
+// ---------------------------------------------------------------- Jacobian fill
+// J block entries of Ybus entry (i, j) in rectangular form (newtonpf.h:97-186):
+//   V_i = a + jb, V_j = c + jd, yv = Y_ij V_j, w = yv / |V_j|, I = Ibus_i if i == j else 0
+//   dP/dVa = -b (I_r - yv_r) - a (-I_i + yv_i)     dP/dVm = a w_r + b w_i + (I_r c + I_i d)/|V_j|
+//   dQ/dVa = -b (-I_i + yv_i) + a (I_r - yv_r)     dQ/dVm = -a w_i + b w_r + (I_r d - I_i c)/|V_j|
+template <typename T>
+__global__ void __launch_bounds__(256) k_jfill(DevGrid d, T* A) {
+  const int g = blockIdx.y;
+  if (!d.group_active[g]) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = g * 32 + lane;
+  LaneOut o;
+  load_outages(d, c, o);
+  const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
+  for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
+    const int i = d.mis_rows[r];
+    const double2 vi = d.V[at32(g, d.nb, i, lane)];
+    const double2 ibus = d.Ibus[at32(g, d.nb, i, lane)];
+    const double a = vi.x, b = vi.y;
+    for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
+      const int4 jp = d.jpos[p];
+      if (jp.x < 0 && jp.y < 0 && jp.z < 0 && jp.w < 0) continue;
+      const int j = d.y_col[p];
+      const double2 y = ycase(d, o, p, d.y_val[p]);
+      const double2 vj = d.V[at32(g, d.nb, j, lane)];
+      const double cc = vj.x, dd = vj.y;
+      const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
+      const double ir = (i == j) ? ibus.x : 0.0, ii = (i == j) ? ibus.y : 0.0;
+      if (jp.x >= 0) A[at32(g, d.nA_jac, jp.x, lane)] = (T)(-b * (ir - yvr) - a * (-ii + yvi));
+      if (jp.z >= 0) A[at32(g, d.nA_jac, jp.z, lane)] = (T)(-b * (-ii + yvi) + a * (ir - yvr));
+      if (jp.y >= 0 || jp.w >= 0) {
+        const double ab = sqrt(cc * cc + dd * dd);
+        const double wr = yvr / ab, wi = yvi / ab;
+        if (jp.y >= 0) A[at32(g, d.nA_jac, jp.y, lane)] = (T)(a * wr + b * wi + (ir * cc + ii * dd) / ab);
+        if (jp.w >= 0) A[at32(g, d.nA_jac, jp.w, lane)] = (T)(-a * wi + b * wr + (ir * dd - ii * cc) / ab);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- Newton update
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_nr(DevGrid d, const T* x) {
+  const int g = blockIdx.y;
+  if (!d.group_active[g]) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = g * 32 + lane;
+  if (d.status[c] != ST_RUNNING) return;
+  const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
+  for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
+    const int i = d.mis_rows[r];
+    const int2 jv = d.jvar[i];
+    const double dva = (double)x[at32(g, d.n_jac, jv.x, lane)];
+    const double dvm = jv.y >= 0 ? (double)x[at32(g, d.n_jac, jv.y, lane)] : 0.0;
+    const size_t k = at32(g, d.nb, i, lane);
+    const double2 v = d.V[k];
+    const double mag = sqrt(v.x * v.x + v.y * v.y) - dvm;
+    const double ang = vangle(v, d.angle_mode) - dva;
+    double sn, cs;
+    sincos(ang, &sn, &cs);
+    d.V[k] = make_double2(mag * cs, mag * sn);
+  }
+}
+
+// ---------------------------------------------------------------- fast decoupled
+struct DevFD {
+  int n_bp, n_bpp;
+  const int2* fdvar;   // [nb] (B' var, B'' var) or -1
+};
+
+// P = Re(mis)/|V| over PV/PQ, Q = Im(mis)/|V| over PQ (fdpf.h:369-414)
+template <typename T>
+__global__ void __launch_bounds__(256) k_mismatch_fd(DevGrid d, DevFD f, T* xp, T* xq) {
+  const int g = blockIdx.y;
+  if (!d.group_active[g]) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = g * 32 + lane;
+  LaneOut o;
+  load_outages(d, c, o);
+  double lmax = 0.0;
+  const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
+  for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
+    const int i = d.mis_rows[r];
+    double2 ib = make_double2(0.0, 0.0);
+    for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
+      const double2 y = ycase(d, o, p, d.y_val[p]);
+      const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
+      ib.x += y.x * v.x - y.y * v.y;
+      ib.y += y.x * v.y + y.y * v.x;
+    }
+    const double2 vi = d.V[at32(g, d.nb, i, lane)];
+    const double2 s = d.sbus_case ? d.sbus_case[at32(g, d.nb, i, lane)] : d.sbus0[i];
+    const double av = sqrt(vi.x * vi.x + vi.y * vi.y);
+    const double mr = (vi.x * ib.x + vi.y * ib.y - s.x) / av;
+    const double mi = (vi.y * ib.x - vi.x * ib.y - s.y) / av;
+    const int2 fv = f.fdvar[i];
+    xp[at32(g, f.n_bp, fv.x, lane)] = (T)mr;
+    double m = fabs(mr);
+    if (mr != mr) m = INFINITY;
+    if (fv.y >= 0) {
+      xq[at32(g, f.n_bpp, fv.y, lane)] = (T)mi;
+      m = fmax(m, fabs(mi));
+      if (mi != mi) m = INFINITY;
+    }
+    lmax = fmax(lmax, finite_or_inf(m));
+  }
+  block_lane_max(lmax, &d.facc[c], d.status[c] == ST_RUNNING);
+}
+
+// half updates (fdpf.h:416-448): Va -= dVa over PV/PQ (half 0), |V| -= dVm over PQ (half 1)
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_fd(DevGrid d, DevFD f, const T* xp, const T* xq, int half) {
+  const int g = blockIdx.y;
+  if (!d.group_active[g]) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = g * 32 + lane;
+  if (d.status[c] != ST_RUNNING) return;
+  const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
+  for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
+    const int i = d.mis_rows[r];
+    const int2 fv = f.fdvar[i];
+    if (half == 1 && fv.y < 0) continue;
+    const size_t k = at32(g, d.nb, i, lane);
+    const double2 v = d.V[k];
+    double mag = sqrt(v.x * v.x + v.y * v.y);
+    double ang = vangle(v, d.angle_mode);
+    if (half == 0) ang -= (double)xp[at32(g, f.n_bp, fv.x, lane)];
+    else mag -= (double)xq[at32(g, f.n_bpp, fv.y, lane)];
+    double sn, cs;
+    sincos(ang, &sn, &cs);
+    d.V[k] = make_double2(mag * cs, mag * sn);
+  }
+}
+
+// B'/B'' values of every case: base arrowhead values, then minus the outaged
+// branches' contributions.  Thread per (entry, lane).
+template <typename T>
+__global__ void k_fd_base(int ngroups, int nA, const double* base, T* A) {
+  const size_t total = (size_t)ngroups * nA * 32;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x)
+    A[t] = (T)base[(t >> 5) % nA];
+}
+
+template <typename T>
+__global__ void k_fd_outage(DevGrid d, int nA, const int4* br_apos, const double4* br_bval, T* A) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.ngroups * 32) return;
+  const int g = c >> 5, lane = c & 31;
+  const int stride = d.ngroups * 32;
+  for (int k = 0; k < kMaxOut; ++k) {
+    const int e = d.out_br[k * stride + c];
+    if (e < 0) continue;
+    const int4 p = br_apos[e];
+    const double4 v = br_bval[e];
+    const int ps[4] = {p.x, p.y, p.z, p.w};
+    const double vs[4] = {v.x, v.y, v.z, v.w};
+    for (int q = 0; q < 4; ++q) {
+      if (ps[q] < 0) continue;
+      const size_t idx = at32(g, nA, ps[q], lane);
+      A[idx] = (T)((double)A[idx] - vs[q]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- multifrontal LU
+// Task = (supernode s, lane chunk of G cases).  A team of TEAM threads holds the
+// front F (f x (f+1), right-hand side in column f) in shared memory as
+// F[(row * (f+1) + col) * G + lane]; SLOTS = TEAM / G threads share each lane.
+//   1. F = 0; scatter the arrowhead (this supernode's J / B entries) and the
+//      right-hand side of its pivot rows;
+//   2. extend-add each child's contribution block (and carried right-hand side);
+//   3. partial LU of the w pivots (no pivoting: diagonal pivots, the reference's
+//      J is factorised in the same static order for every case);
+//   4. store the U- and L-panels, the forward-substituted y of the pivots, and
+//      the contribution block for the parent.
+template <int TEAM>
+__device__ __forceinline__ void team_sync() {
+  if (TEAM == 32) __syncwarp();
+  else __syncthreads();
+}
+
+template <typename T, int G, int TEAM>
+__global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
+    DevLU L, const int* __restrict__ task_sn, int nsn_l, int ngroups, int fcap,
+    const T* __restrict__ A, T* __restrict__ pan, T* __restrict__ cb, T* __restrict__ cbr,
+    T* __restrict__ x, int* __restrict__ status, const int* __restrict__ group_active, int with_rhs) {
+  constexpr int SLOTS = TEAM / G;
+  constexpr int LPG = 32 / G;  // lane chunks per group
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int teams = blockDim.x / TEAM;
+  const int team = threadIdx.x / TEAM, tid = threadIdx.x % TEAM;
+  const int slot = tid / G, l = tid % G;
+  T* F = reinterpret_cast<T*>(smem_raw) + (size_t)team * fcap * (fcap + 1) * G;
+  const long long nchunks = (long long)ngroups * LPG;
+  const long long ntasks = (long long)nsn_l * nchunks;
+  for (long long t = (long long)blockIdx.x * teams + team; t < ntasks; t += (long long)gridDim.x * teams) {
+    const int s = task_sn[t / nchunks];
+    const int ch = (int)(t % nchunks);
+    const int g = ch / LPG;
+    if (!group_active[g]) continue;
+    const int lane = (ch % LPG) * G + l;
+    const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s];
+    const int f1 = f + 1;
+    for (int idx = slot; idx < f * f1; idx += SLOTS) F[idx * G + l] = (T)0;
+    team_sync<TEAM>();
+    for (int e = L.ah_ptr[s] + slot; e < L.ah_ptr[s + 1]; e += SLOTS)
+      F[L.ah_loc[e] * G + l] = A[at32(g, L.nA, e, lane)];
+    if (with_rhs)
+      for (int p = slot; p < w; p += SLOTS) F[(p * f1 + f) * G + l] = x[at32(g, L.n, c0 + p, lane)];
+    team_sync<TEAM>();
+    for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
+      const int ch2 = L.child_list[ci];
+      const int m = L.sn_f[ch2] - (L.sn_c0[ch2 + 1] - L.sn_c0[ch2]);
+      const int* rel = L.relmap + L.rel_ptr[ch2];
+      const long long cbo = L.cb_off[ch2];
+      for (int idx = slot; idx < m * m; idx += SLOTS) {
+        const int a = idx / m, b = idx - a * m;
+        F[(rel[a] * f1 + rel[b]) * G + l] += cb[at32(g, L.sumcb, cbo + idx, lane)];
+      }
+      if (with_rhs)
+        for (int a = slot; a < m; a += SLOTS)
+          F[(rel[a] * f1 + f) * G + l] += cbr[at32(g, L.sumcbr, L.cbr_off[ch2] + a, lane)];
+      team_sync<TEAM>();
+    }
+    const int ncol_extra = with_rhs ? 1 : 0;
+    for (int p = 0; p < w; ++p) {
+      T piv = F[(p * f1 + p) * G + l];
+      if (!(fabs((double)piv) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)piv) <= DBL_MAX)) {
+        if (slot == 0) status[g * 32 + lane] = ST_SINGULAR;
+        piv = (T)1;
+      }
+      const T inv = (T)1 / piv;
+      for (int i = p + 1 + slot; i < f; i += SLOTS) F[(i * f1 + p) * G + l] *= inv;
+      team_sync<TEAM>();
+      const int nrow = f - p - 1, ncol = f - p - 1 + ncol_extra;
+      for (int idx = slot; idx < nrow * ncol; idx += SLOTS) {
+        const int i = p + 1 + idx / ncol, q = p + 1 + idx % ncol;
+        F[(i * f1 + q) * G + l] -= F[(i * f1 + p) * G + l] * F[(p * f1 + q) * G + l];
+      }
+      team_sync<TEAM>();
+    }
+    const long long po = L.pan_off[s];
+    for (int idx = slot; idx < w * f; idx += SLOTS) {
+      const int p = idx / f, q = idx - p * f;
+      pan[at32(g, L.nnz, po + idx, lane)] = F[(p * f1 + q) * G + l];
+    }
+    const int m = f - w;
+    for (int idx = slot; idx < m * w; idx += SLOTS) {
+      const int i = w + idx / w, q = idx % w;
+      pan[at32(g, L.nnz, po + (long long)w * f + idx, lane)] = F[(i * f1 + q) * G + l];
+    }
+    if (with_rhs)
+      for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, c0 + p, lane)] = F[(p * f1 + f) * G + l];
+    if (L.sn_parent[s] >= 0) {
+      const long long cbo = L.cb_off[s];
+      for (int idx = slot; idx < m * m; idx += SLOTS) {
+        const int a = idx / m, b = idx - a * m;
+        cb[at32(g, L.sumcb, cbo + idx, lane)] = F[((w + a) * f1 + w + b) * G + l];
+      }
+      if (with_rhs)
+        for (int a = slot; a < m; a += SLOTS)
+          cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = F[((w + a) * f1 + f) * G + l];
+    }
+    team_sync<TEAM>();
+  }
+}
+
+// Forward substitution with stored factors (fast-decoupled solves): thread per
+// case, warp per (supernode, group).  b accumulates in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(128) k_mf_fsolve(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+                                                   int ngroups, int fcap, const T* __restrict__ pan,
+                                                   T* __restrict__ cbr, T* __restrict__ x,
+                                                   const int* __restrict__ group_active) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  T* b = reinterpret_cast<T*>(smem_raw) + (size_t)warp * fcap * 32;
+  const long long ntasks = (long long)nsn_l * ngroups;
+  for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
+    const int s = task_sn[t / ngroups];
+    const int g = (int)(t % ngroups);
+    if (!group_active[g]) continue;
+    const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s];
+    for (int i = 0; i < f; ++i) b[i * 32 + lane] = (T)0;
+    for (int p = 0; p < w; ++p) b[p * 32 + lane] = x[at32(g, L.n, c0 + p, lane)];
+    for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
+      const int ch = L.child_list[ci];
+      const int m = L.sn_f[ch] - (L.sn_c0[ch + 1] - L.sn_c0[ch]);
+      const int* rel = L.relmap + L.rel_ptr[ch];
+      for (int a = 0; a < m; ++a) b[rel[a] * 32 + lane] += cbr[at32(g, L.sumcbr, L.cbr_off[ch] + a, lane)];
+    }
+    const long long po = L.pan_off[s];
+    for (int p = 0; p < w; ++p) {
+      const T yp = b[p * 32 + lane];
+      for (int i = p + 1; i < w; ++i) b[i * 32 + lane] -= pan[at32(g, L.nnz, po + (long long)i * f + p, lane)] * yp;
+      for (int i = w; i < f; ++i)
+        b[i * 32 + lane] -= pan[at32(g, L.nnz, po + (long long)w * f + (long long)(i - w) * w + p, lane)] * yp;
+    }
+    for (int p = 0; p < w; ++p) x[at32(g, L.n, c0 + p, lane)] = b[p * 32 + lane];
+    if (L.sn_parent[s] >= 0)
+      for (int a = 0; a < f - w; ++a) cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = b[(w + a) * 32 + lane];
+    __syncwarp();
+  }
+}
+
+// Backward substitution: thread per case, warp per (supernode, group); ancestors'
+// solutions are final (previous launches), the pivots' own are solved in order.
+template <typename T>
+__global__ void __launch_bounds__(128) k_mf_bsolve(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+                                                   int ngroups, const T* __restrict__ pan, T* __restrict__ x,
+                                                   const int* __restrict__ group_active) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  const long long ntasks = (long long)nsn_l * ngroups;
+  for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
+    const int s = task_sn[t / ngroups];
+    const int g = (int)(t % ngroups);
+    if (!group_active[g]) continue;
+    const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s];
+    const int* rows = L.sn_rows + L.sn_rptr[s];
+    const long long po = L.pan_off[s];
+    for (int p = w - 1; p >= 0; --p) {
+      T acc = x[at32(g, L.n, c0 + p, lane)];
+      const T* urow = pan;  // U-panel row p: entries (p, q), q = 0..f-1
+      for (int q = p + 1; q < f; ++q)
+        acc -= urow[at32(g, L.nnz, po + (long long)p * f + q, lane)] * x[at32(g, L.n, rows[q], lane)];
+      x[at32(g, L.n, c0 + p, lane)] = acc / urow[at32(g, L.nnz, po + (long long)p * f + p, lane)];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- results
+// [group][bus][32] -> [case][bus]
+__global__ void k_gather_v(int nb, int ncases, const double2* V, double2* out) {
+  const size_t total = (size_t)ncases * nb;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t / nb), i = (int)(t % nb);
+    out[t] = V[at32(c >> 5, nb, i, c & 31)];
+  }
+}
+
+__global__ void k_gather_small(int ncases, const int* status, const int* iters, const double* maxmis,
+                               uint8_t* st_out, int* it_out, double* mm_out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncases) return;
+  if (st_out) st_out[c] = (uint8_t)status[c];
+  if (it_out) it_out[c] = iters[c];
+  if (mm_out) mm_out[c] = maxmis[c];
+}
+
+}  // namespace mpfk

@@ -1,0 +1,153 @@
+"""Host-side mirror of the reference's power-flow entry points, over libmpf.so.
+
+Reference (src/powerflow/runpf.h):
+  hybrid_init(topology, nTest, nThreads, estrutura, algPF)   runpf.h:795
+  hybrid_runpf(estrutura, enxame)                             runpf.h:606
+  hybrid_free()                                               runpf.h:984
+  mkl_runpf(estrutura, particula) -> loss or DBL_MAX          runpf.h:259
+with algorithms NR / FDXB / FDBX (runpf.h:16-18) and MAX_IT_NR / MAX_IT_FD / EPS
+(runpf.h:45-47).  The reference keeps one global engine per process and exits
+on error; here an engine is an object and errors raise MpfError.
+
+A "case" is the base grid with a list of outaged branches (N-1, N-k: at most 4
+per case) and, optionally, its own bus injections.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _types as T
+from ._lib import MpfError, lib, ptr
+from .grid import cases_to_offsets
+
+NR, FDXB, FDBX = T.NR, T.FDXB, T.FDBX
+FP64, MIXED = T.FP64, T.MIXED
+MAX_IT_NR, MAX_IT_FD, EPS = T.MAX_IT_NR, T.MAX_IT_FD, T.EPS
+
+CONVERGED = T.CASE_CONVERGED
+
+
+class Results:
+    """Per-case outputs: v (n_cases, n_bus) complex, iterations, status, max_mis."""
+
+    def __init__(self, v, iterations, status, max_mis):
+        self.v = v
+        self.iterations = iterations
+        self.status = status
+        self.max_mis = max_mis
+
+    @property
+    def converged(self):
+        return self.status == T.CASE_CONVERGED
+
+
+class PowerFlow:
+    """One grid on one GPU (mpf_create).  Replaces hybrid_init / hybrid_free."""
+
+    def __init__(self, buses, branches, max_it_nr=MAX_IT_NR, max_it_fd=MAX_IT_FD, tol=EPS,
+                 angle_mode=0, device=0):
+        self.buses = np.ascontiguousarray(buses, dtype=T.BUS_DTYPE)
+        self.branches = np.ascontiguousarray(branches, dtype=T.BRANCH_DTYPE)
+        opt = T.Options()
+        lib().mpf_default_options(ctypes.byref(opt))
+        opt.max_it_nr, opt.max_it_fd, opt.tol = max_it_nr, max_it_fd, tol
+        opt.angle_mode, opt.device = angle_mode, device
+        h = ctypes.c_void_p()
+        rc = lib().mpf_create(ptr(self.buses), len(self.buses), ptr(self.branches), len(self.branches),
+                              ctypes.byref(opt), ctypes.byref(h))
+        self._h = h
+        if rc != 0:
+            msg = lib().mpf_last_error(h).decode() if h.value else lib().mpf_status_string(rc).decode()
+            if h.value:
+                lib().mpf_destroy(h)
+                self._h = None
+            raise MpfError(rc, msg)
+        self.n_cases = 0
+
+    # -- lifecycle -----------------------------------------------------------
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib().mpf_destroy(self._h)
+        self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise MpfError(rc, lib().mpf_last_error(self._h).decode())
+
+    # -- cases and solves ----------------------------------------------------
+    def set_cases(self, cases, sbus=None):
+        """cases: list of outage lists (branch indices); sbus: (n_cases, n_bus, 2) or None."""
+        offs, flat = cases_to_offsets(cases)
+        sb = None if sbus is None else np.ascontiguousarray(sbus, dtype=np.float64)
+        self._check(lib().mpf_set_cases(self._h, len(cases), ptr(offs), ptr(flat), ptr(sb)))
+        self.n_cases = len(cases)
+
+    def solve(self, alg=NR, precision=FP64, stream=None):
+        self._check(lib().mpf_solve(self._h, alg, precision, stream))
+
+    def results(self):
+        nb = len(self.buses)
+        v = np.zeros((self.n_cases, nb, 2))
+        it = np.zeros(self.n_cases, np.int32)
+        st = np.zeros(self.n_cases, np.uint8)
+        mm = np.zeros(self.n_cases)
+        self._check(lib().mpf_get_results(self._h, ptr(v), ptr(it), ptr(st), ptr(mm)))
+        return Results(v[..., 0] + 1j * v[..., 1], it, st, mm)
+
+    def runpf(self, cases, alg=NR, precision=FP64, sbus=None):
+        """End to end from host memory (mpf_runpf_host): cases in, results out."""
+        nb = len(self.buses)
+        n = len(cases)
+        offs, flat = cases_to_offsets(cases)
+        sb = None if sbus is None else np.ascontiguousarray(sbus, dtype=np.float64)
+        v = np.zeros((n, nb, 2))
+        it = np.zeros(n, np.int32)
+        st = np.zeros(n, np.uint8)
+        mm = np.zeros(n)
+        self._check(lib().mpf_runpf_host(self._h, alg, precision, n, ptr(offs), ptr(flat), ptr(sb),
+                                         ptr(v), ptr(it), ptr(st), ptr(mm)))
+        self.n_cases = n
+        return Results(v[..., 0] + 1j * v[..., 1], it, st, mm)
+
+    def timing(self):
+        t = T.Timing()
+        self._check(lib().mpf_get_timing(self._h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in T.Timing._fields_}
+
+    def stats(self):
+        s = T.Stats()
+        self._check(lib().mpf_get_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in T.Stats._fields_}
+
+
+# -- the reference's procedural names ------------------------------------------
+def hybrid_init(buses, branches, n_tests, alg=NR, **kw):
+    """hybrid_init (runpf.h:795): build the engine for n_tests simultaneous cases."""
+    pf = PowerFlow(buses, branches, **kw)
+    pf.alg = alg
+    pf.n_tests = n_tests
+    return pf
+
+
+def hybrid_runpf(pf, cases, precision=FP64, sbus=None):
+    """hybrid_runpf (runpf.h:606): solve every case; returns Results."""
+    if len(cases) != pf.n_tests:
+        raise ValueError(f"expected {pf.n_tests} cases, got {len(cases)}")
+    return pf.runpf(cases, alg=pf.alg, precision=precision, sbus=sbus)
+
+
+def hybrid_free(pf):
+    """hybrid_free (runpf.h:984)."""
+    pf.close()

@@ -1,0 +1,145 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle.
+
+Tolerances: converged cases must satisfy the reference's own criterion
+max |F| < 1e-8 p.u. (newtonpf.h:394,518); flags must match exactly; plain FP64
+Newton iteration counts must match exactly and mixed precision may take at most
+one more; voltages must agree with the oracle to 1e-8 p.u. (both are converged
+to < 1e-8 mismatch, so agreement is bounded by the conditioning of J).
+"""
+import numpy as np
+import pytest
+
+import mapol_b200 as m
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+V_TOL = 1e-8
+
+
+def _oracle(buses, branches, cases, alg, sbus=None):
+    return oracle.runpf(buses, branches, cases, alg=alg, sbus=sbus)
+
+
+def _compare(res, ref, max_extra_iter=0, v_tol=V_TOL):
+    conv = res.status == m.runpf.CONVERGED
+    assert np.array_equal(conv, ref["converged"]), (np.where(conv != ref["converged"]), res.status)
+    assert (res.max_mis[conv] < 1e-8).all()
+    d_it = res.iterations[conv] - ref["iterations"][conv]
+    assert (d_it >= 0).all() and (d_it <= max_extra_iter).all(), (res.iterations, ref["iterations"])
+    if conv.any():
+        dv = np.abs(res.v[conv] - ref["v"][conv]).max()
+        assert dv < v_tol, dv
+    return conv
+
+
+@pytest.mark.parametrize("name", ["cfg0_30bus", "cfg1_300bus"])
+def test_nr_fp64_matches_oracle(gpu, name):
+    buses, branches, cases = m.workload(name)
+    ref = _oracle(buses, branches, cases, m.NR)
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.FP64)
+        res = pf.results()
+    conv = _compare(res, ref)
+    assert conv.mean() > 0.9
+
+
+@pytest.mark.parametrize("alg", [m.FDXB, m.FDBX])
+@pytest.mark.parametrize("name", ["cfg0_30bus", "cfg1_300bus"])
+def test_fd_fp64_matches_oracle(gpu, name, alg):
+    buses, branches, cases = m.workload(name)
+    ref = _oracle(buses, branches, cases, alg)
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(alg, m.FP64)
+        res = pf.results()
+    _compare(res, ref, v_tol=1e-7)
+
+
+@pytest.mark.parametrize("name", ["cfg0_30bus", "cfg1_300bus"])
+def test_nr_mixed_at_most_one_extra_iteration(gpu, name):
+    buses, branches, cases = m.workload(name)
+    ref = _oracle(buses, branches, cases, m.NR)
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.MIXED)
+        res = pf.results()
+    _compare(res, ref, max_extra_iter=1)
+
+
+def test_runpf_host_end_to_end(gpu):
+    buses, branches, cases = m.workload("cfg1_300bus")
+    ref = _oracle(buses, branches, cases, m.NR)
+    pf = m.hybrid_init(buses, branches, len(cases), m.NR)
+    res = m.hybrid_runpf(pf, cases)
+    m.hybrid_free(pf)
+    _compare(res, ref)
+
+
+@pytest.mark.parametrize("n_bus,n_branch,n_pv,n_out", [(118, 179, 53, 64), (1354, 1991, 259, 40)])
+def test_uneven_sizes_match_oracle(gpu, n_bus, n_branch, n_pv, n_out):
+    buses, branches = m.synth_grid(n_bus, n_branch, n_pv, 0.1, seed=2)
+    cases = m.n1_cases(branches, n_bus, n_out, 5, with_base=True)
+    ref = _oracle(buses, branches, cases, m.NR)
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.FP64)
+        _compare(pf.results(), ref)
+
+
+def test_n2_outages_and_load_scenarios(gpu):
+    buses, branches = m.synth_grid(300, 411, 69, 0.1, seed=4)
+    out = m.select_outages(branches, 300, 40, 9)
+    cases = [[int(out[2 * k]), int(out[2 * k + 1])] for k in range(20)] + [[]] * 4
+    sbus = m.load_scenarios(buses, len(cases), 0.05, 3)
+    ref = _oracle(buses, branches, cases, m.NR, sbus=sbus)
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases, sbus=sbus)
+        pf.solve(m.NR, m.FP64)
+        _compare(pf.results(), ref)
+
+
+def test_batch_not_multiple_of_32_and_repeated_solves(gpu):
+    buses, branches, cases = m.workload("cfg1_300bus")
+    cases = cases[:45]
+    ref = _oracle(buses, branches, cases, m.NR)
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        for alg in (m.NR, m.FDXB, m.NR):
+            pf.solve(alg, m.FP64)
+        _compare(pf.results(), ref)
+
+
+def test_bridge_outage_is_reported_not_converged(gpu):
+    buses, branches = m.synth_grid(300, 411, 69, 0.1, seed=1)
+    bridges = np.where(m.find_bridges(branches, 300))[0]
+    cases = [[int(bridges[0])], []]
+    ref = _oracle(buses, branches, cases, m.NR)
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.FP64)
+        res = pf.results()
+    assert res.status[1] == m.runpf.CONVERGED
+    assert res.status[0] != m.runpf.CONVERGED
+    assert not ref["converged"][0]
+
+
+def test_bad_inputs_raise_not_crash(gpu):
+    buses, branches = m.synth_grid(30, 41, 5)
+    with m.PowerFlow(buses, branches) as pf:
+        with pytest.raises(m.MpfError):
+            pf.solve(m.NR, m.FP64)  # before set_cases
+        with pytest.raises(m.MpfError):
+            pf.set_cases([[1000]])
+        with pytest.raises(m.MpfError):
+            pf.set_cases([[1, 1]])
+        with pytest.raises(m.MpfError):
+            pf.set_cases([[1, 2, 3, 4, 5]])
+        pf.set_cases([[]])
+        with pytest.raises(m.MpfError):
+            pf.solve(7, m.FP64)
+    bad = buses.copy()
+    bad["type"][bad["type"] == 3] = 1
+    with pytest.raises(m.MpfError):
+        m.PowerFlow(bad, branches)
