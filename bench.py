@@ -1,0 +1,369 @@
+"""Benchmark: N-1 power-flow solves/s on the 9241-bus synthetic grid (1000 N-1
+contingencies, Newton-Raphson to 1e-8 p.u.), mixed precision vs plain FP64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one batched solve of every case of the workload, from the flat start to
+convergence.  ours: prints one JSON line (rank 0) with value = mixed-precision
+solves/s (all ranks), plain FP64 beside it, per-kernel roofline of the dominant
+kernel, the end-to-end figure through the host C-ABI call, the CPU baseline and
+the GPU clocks seen during the timed region.  reference: times the reference's
+own CPU implementation of the path (its Eigen SparseLU option, the oracle build
+compiled against the reference's vendored Eigen) on this host's cores.
+
+Multi-GPU: one process per GPU (torchrun); each rank solves its own 1000-case
+N-1 set of the same grid (weak scaling, no data-path collective); the time is
+the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "cfg3_9241bus"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[4 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU baselines
+def cpu_port_baseline(buses, branches, cases, budget_s=15.0):
+    """The oracle (own sparse LU, all host threads) on a bounded sample of the cases."""
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    n = min(len(cases), max(threads, 8))
+    t = time.perf_counter()
+    r = oracle.runpf(buses, branches, cases[:n], alg=0, solver=oracle.SOLVER_GP, threads=threads)
+    dt = time.perf_counter() - t
+    # grow the sample toward the time budget
+    if dt < budget_s / 4 and n < len(cases):
+        n2 = min(len(cases), int(n * budget_s / 2 / max(dt, 1e-3)))
+        t = time.perf_counter()
+        r = oracle.runpf(buses, branches, cases[:n2], alg=0, solver=oracle.SOLVER_GP, threads=threads)
+        dt = time.perf_counter() - t
+        n = n2
+    return {"value": n / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{n} of the {len(cases)} N-1 cases, NR FP64 to 1e-8, oracle sparse LU "
+                      f"(Gilbert-Peierls, minimum degree), {threads} threads, {dt:.1f} s",
+            "converged": int(r["converged"].sum())}
+
+
+def reference_arm(args):
+    """Reference's own CPU path on this host: the NR of mkl_newtonpf with the
+    reference's Eigen SparseLU option (newtonpf.h:341-363, compute() every solve),
+    from the oracle build compiled against the reference's vendored Eigen."""
+    import mapol_b200 as m
+    from oracle import oracle
+
+    buses, branches, cases = m.workload(args.workload)
+    if not oracle.has_eigen():
+        return {"impl": "reference", "unavailable": "oracle/_ref (reference Eigen build) not present"}
+    threads = os.cpu_count() or 1
+    sample = cases[:threads]
+    # iterations each case needs (own solver, same arithmetic path apart from the LU)
+    it_ref = oracle.runpf(buses, branches, sample, alg=0, solver=oracle.SOLVER_GP, threads=threads)["iterations"]
+    iters = float(np.mean(it_ref))
+
+    def step():
+        # one Newton iteration of every sampled case (max_it = 1), one case per thread
+        t = time.perf_counter()
+        oracle.runpf(buses, branches, sample, alg=0, max_it=1, solver=oracle.SOLVER_EIGEN, threads=threads)
+        return time.perf_counter() - t
+
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    per_step = sum(times) / len(times)
+    value = len(sample) / (iters * per_step)
+    return {
+        "impl": "reference", "metric": "N-1 PF solves/sec @1e-8 pu, 9241-bus synth", "value": value,
+        "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": args.workload, "n_cases_sample": len(sample), "alg": "NR",
+                   "linear_solver": "Eigen 3.2.8 SparseLU<COLAMD> (reference's Eigen_SparseLU option)"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference",
+                         "sample": f"each step = one Newton iteration of {len(sample)} cases (one per thread); "
+                                   f"solves/s = cases / ({iters:.1f} iterations x step time)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import mapol_b200 as m
+    from mapol_b200 import _types as T
+    from mapol_b200._lib import lib, ptr
+    from mapol_b200.grid import cases_to_offsets
+
+    torch.cuda.set_device(local_rank)
+    buses, branches, _ = m.workload(args.workload)
+    w = m.WORKLOADS[args.workload]
+    cases = m.n1_cases(branches, w["n_bus"], w["n_out"], 7 + rank, w["with_base"])
+    n_cases = len(cases)
+    pf = m.PowerFlow(buses, branches, device=local_rank)
+    pf.set_cases(cases)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    out = {}
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    for prec, name in ((m.MIXED, "mixed"), (m.FP64, "fp64")):
+        for _ in range(args.warmup):
+            pf.solve(m.NR, prec, stream.cuda_stream)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fam = {k: 0.0 for k in ("mismatch_ms", "jacobian_ms", "factor_ms", "solve_ms", "update_ms", "other_ms")}
+        launches, iters_sum, nfact = 0, 0, 0
+        e0.record(stream)
+        for _ in range(args.steps):
+            pf.solve(m.NR, prec, stream.cuda_stream)
+            tm = pf.timing()
+            for k in fam:
+                fam[k] += tm[k]
+            launches += tm["launches"]
+            nfact += tm["iterations_max"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        res = pf.results()
+        conv = res.status == T.CASE_CONVERGED
+        iters_sum = int(res.iterations[conv].sum())
+        out[name] = dict(ms=ms, fam={k: v / args.steps for k, v in fam.items()}, launches=launches,
+                         n_conv=int(conv.sum()), iters=np.bincount(res.iterations, minlength=11).tolist(),
+                         max_mis=float(res.max_mis[conv].max()) if conv.any() else None,
+                         iters_sum=iters_sum, nfact=nfact / args.steps)
+    clocks = sampler.stop() if sampler else None
+    st = pf.stats()  # after the solves: device_bytes includes the factor buffers
+
+    # end to end through the host C-ABI call: case definitions in from pinned host
+    # memory, voltages / flags / iterations / mismatch back into pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        offs, flat = cases_to_offsets(cases)
+        nb = len(buses)
+        offs_t = torch.from_numpy(offs).pin_memory()
+        flat_t = torch.from_numpy(flat).pin_memory()
+        v_t = torch.empty((n_cases, nb, 2), dtype=torch.float64).pin_memory()
+        it_t = torch.empty(n_cases, dtype=torch.int32).pin_memory()
+        st_t = torch.empty(n_cases, dtype=torch.uint8).pin_memory()
+        mm_t = torch.empty(n_cases, dtype=torch.float64).pin_memory()
+        L = lib()
+
+        def call():
+            rc = L.mpf_runpf_host(pf._h, m.NR, m.MIXED, n_cases, offs_t.data_ptr(), flat_t.data_ptr(), None,
+                                  v_t.data_ptr(), it_t.data_ptr(), st_t.data_ptr(), mm_t.data_ptr())
+            if rc != 0:
+                raise RuntimeError(L.mpf_last_error(pf._h).decode())
+
+        for _ in range(args.warmup):
+            call()
+        torch.cuda.synchronize()
+        barrier()
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            call()
+        dt = max_over_ranks(time.perf_counter() - t)
+        barrier()
+        h2d = offs.nbytes + flat.nbytes
+        d2h = v_t.numel() * 8 + n_cases * (4 + 1 + 8)
+        e2e = {"value": n_cases * world * args.steps / dt, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "precision": "mixed",
+               "n_converged": int((st_t.numpy() == T.CASE_CONVERGED).sum())}
+    pf.close()
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    mixed, fp64 = out["mixed"], out["fp64"]
+    value = n_cases * world * args.steps / (mixed["ms"] / 1e3)
+    value_fp64 = n_cases * world * args.steps / (fp64["ms"] / 1e3)
+
+    # roofline of the dominant kernel family of the headline (mixed) solve.
+    # Algorithmic bytes per case per Newton iteration (w = bytes per LU value):
+    #   factor:   2 w nnz(L+U)            solve: w nnz(L+U) + 3*8*n
+    #   mismatch: 16 nb (V) + 16 nb (Sbus) + 8 n (F)     jacobian: 16 nb + w nnz(J)
+    #   update:   8 n + 32 nb
+    def alg_bytes(family, w_lu):
+        nb, n, nnz_lu, nnz_j = st["n_bus"], st["n_jac"], st["nnz_lu"], st["nnz_jac"]
+        return {"factor_ms": 2 * w_lu * nnz_lu, "solve_ms": w_lu * nnz_lu + 24 * n,
+                "mismatch_ms": 32 * nb + 8 * n, "jacobian_ms": 16 * nb + w_lu * nnz_j,
+                "update_ms": 8 * n + 32 * nb}.get(family)
+
+    fams = {k: v for k, v in mixed["fam"].items() if k != "other_ms"}
+    dom = max(fams, key=fams.get)
+    # units processed per step by that family: Newton iterations summed over cases
+    units = mixed["iters_sum"]
+    achieved = alg_bytes(dom, 4) * units / (fams[dom] / 1e3) / 1e9
+    per_family = {}
+    for k, v in fams.items():
+        b = alg_bytes(k, 4)
+        per_family[k.replace("_ms", "")] = {"ms_per_step": round(v, 4),
+                                            "GB/s": round(b * units / (v / 1e3) / 1e9, 1) if v > 0 else None}
+
+    line = {
+        "metric": "N-1 PF solves/sec @1e-8 pu, 9241-bus synth: mixed vs plain FP64; HBM GB/s",
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mixed["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 mismatch/update/convergence test, f32 LU factorisation and solves",
+        "data": "synthetic (seeded generator: 9241 buses, 16049 branches, 1445 PV, 15% tapped)",
+        "config": {"workload": f"{args.workload}: {n_cases} N-1 contingencies per GPU, NR to 1e-8 p.u.",
+                   "n_cases_per_gpu": n_cases, "alg": "NR", "parallelism": f"replicas x{world} (cases sharded)",
+                   "l2": "inputs larger than L2 (factor working set %.1f GB per GPU)" % (st["device_bytes"] / 1e9)},
+        "plain_fp64": {"value": value_fp64, "ms_per_step": fp64["ms"] / args.steps,
+                       "converged": fp64["n_conv"], "iterations_hist": fp64["iters"],
+                       "max_mismatch": fp64["max_mis"]},
+        "mixed_over_plain": value / value_fp64,
+        "mixed": {"converged": mixed["n_conv"], "iterations_hist": mixed["iters"], "max_mismatch": mixed["max_mis"]},
+        "roofline": {"bound": "hbm", "kernel": dom.replace("_ms", ""), "achieved": round(achieved, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "per_family": per_family},
+        "gpu_launches": int(mixed["launches"]),
+        "clocks": clocks,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_port_baseline(buses, branches, cases)
+    return line
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

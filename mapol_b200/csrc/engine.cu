@@ -65,10 +65,12 @@ struct DevBuf {
   T* as() const { return reinterpret_cast<T*>(p); }
 };
 
+// Copies v to the device, reusing b's allocation when it is large enough.
 template <class T>
 void upload(DevBuf& b, const std::vector<T>& v) {
-  b.alloc(v.size() * sizeof(T));
-  if (!v.empty()) CUDA_TRY(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  const size_t need = v.size() * sizeof(T);
+  if (!b.p || b.bytes < need) b.alloc(need);
+  if (!v.empty()) CUDA_TRY(cudaMemcpy(b.p, v.data(), need, cudaMemcpyHostToDevice));
 }
 
 // ------------------------------------------------------------------ LU system

@@ -143,3 +143,26 @@ def test_bad_inputs_raise_not_crash(gpu):
     bad["type"][bad["type"] == 3] = 1
     with pytest.raises(m.MpfError):
         m.PowerFlow(bad, branches)
+
+
+def test_full_size_9241_bus_sample_matches_oracle(gpu):
+    """The 9241-bus workload (all 1000 cases solved on the GPU), with 48 of them
+    checked against the oracle and every case checked by its own mismatch."""
+    buses, branches, cases = m.workload("cfg3_9241bus")
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.FP64)
+        res = pf.results()
+        pf.solve(m.NR, m.MIXED)
+        res_mixed = pf.results()
+    conv = res.status == m.runpf.CONVERGED
+    assert conv.mean() > 0.95
+    assert (res.max_mis[conv] < 1e-8).all()
+    conv_m = res_mixed.status == m.runpf.CONVERGED
+    assert np.array_equal(conv, conv_m)
+    assert (res_mixed.iterations[conv] <= res.iterations[conv] + 1).all()
+    assert np.abs(res_mixed.v[conv] - res.v[conv]).max() < 1e-7
+    idx = np.linspace(0, len(cases) - 1, 48).astype(int)
+    ref = _oracle(buses, branches, [cases[i] for i in idx], m.NR)
+    sub = type(res)(res.v[idx], res.iterations[idx], res.status[idx], res.max_mis[idx])
+    _compare(sub, ref)
