@@ -329,6 +329,7 @@ struct mpf_handle {
   int ncases = 0, ngroups = 0, maxk = 0;
   DevBuf out_br, sbus_case, V, Ibus, status, iters, maxmis, facc, group_active, any_active;
   DevBuf vout, small_out;
+  DevBuf eval_acc;  // mpf_mismatch accumulator, allocated on first use
   bool have_cases = false, have_results = false;
   int last_alg = -1, last_prec = -1;
   cudaStream_t last_stream = nullptr;  // stream of the last solve / result copy
@@ -372,7 +373,7 @@ struct mpf_handle {
     size_t b = 0;
     const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
                            &out_br, &sbus_case, &V, &Ibus, &status, &iters, &maxmis, &facc, &group_active,
-                           &any_active, &vout, &small_out, &fdvar};
+                           &any_active, &vout, &small_out, &fdvar, &eval_acc};
     for (auto p : all) b += p->bytes;
     const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
     for (auto s : systems) {
@@ -909,6 +910,29 @@ int32_t mpf_get_results(mpf_handle* h, double* v, int32_t* iterations, uint8_t* 
     if (max_mis) CUDA_TRY(cudaMemcpyAsync(max_mis, d_mm, h->ncases * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (status) CUDA_TRY(cudaMemcpyAsync(status, d_st, h->ncases, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_mismatch(mpf_handle* h, const double* v, double* max_mis, void* stream) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (!h->have_cases) return fail(h, MPF_ERR_STATE, "mpf_set_cases must be called before mpf_mismatch");
+  if (!v || !max_mis) return fail(h, MPF_ERR_BAD_INPUT, "v and max_mis must be device pointers");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->own_stream;
+    const size_t need = (size_t)h->ncases * sizeof(unsigned long long);
+    if (!h->eval_acc.p || h->eval_acc.bytes < need) {
+      h->eval_acc.alloc(need);
+      CUDA_TRY(cudaMemset(h->eval_acc.p, 0, need));
+    }
+    const int nfree = (int)h->g.mis_rows.size();
+    k_mismatch_eval<<<dim3((unsigned)((nfree + 255) / 256), (unsigned)h->ncases), 256, 0, st>>>(
+        h->dev(), reinterpret_cast<const double2*>(v), h->ncases, h->eval_acc.as<unsigned long long>());
+    CUDA_TRY(cudaGetLastError());
+    k_acc_drain<<<(h->ncases + 255) / 256, 256, 0, st>>>(h->eval_acc.as<unsigned long long>(), max_mis, h->ncases);
+    CUDA_TRY(cudaGetLastError());
+    h->last_stream = st;
     return MPF_OK;
   });
 }

@@ -552,6 +552,55 @@ __global__ void __launch_bounds__(128) k_mf_bsolve(DevLU L, const int* __restric
   }
 }
 
+// ---------------------------------------------------------------- mismatch of given voltages
+// max |F| per case for voltages given case-major (v[c][i], the layout results use),
+// F = [Re mis_pv; Re mis_pq; Im mis_pq] as newtonpf.h:18-71 (hybrid_checkConvergence,
+// newtonpf.h:526-568, plus the host max loop of newtonpf.h:1241-1254).
+// Grid (row blocks of 256, cases); a warp covers 32 mismatch rows of one case and
+// folds them with shuffles, then one atomicMax per warp into acc[c].
+__global__ void __launch_bounds__(256) k_mismatch_eval(DevGrid d, const double2* __restrict__ v, int ncases,
+                                                       unsigned long long* __restrict__ acc) {
+  const int c = blockIdx.y;
+  if (c >= ncases) return;
+  LaneOut o;
+  load_outages(d, c, o);
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (r < d.nfree) {
+    const double2* vc = v + (size_t)c * d.nb;
+    const int i = d.mis_rows[r];
+    double2 ib = make_double2(0.0, 0.0);
+    for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
+      const double2 y = ycase(d, o, p, d.y_val[p]);
+      const double2 vj = vc[d.y_col[p]];
+      ib.x += y.x * vj.x - y.y * vj.y;
+      ib.y += y.x * vj.y + y.y * vj.x;
+    }
+    const double2 vi = vc[i];
+    const double2 s = d.sbus_case ? d.sbus_case[at32(c >> 5, d.nb, i, c & 31)] : d.sbus0[i];
+    const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
+    const double mi = vi.y * ib.x - vi.x * ib.y - s.y;
+    m = fabs(mr);
+    if (mr != mr) m = INFINITY;
+    if (d.jvar[i].y >= 0) {
+      m = fmax(m, fabs(mi));
+      if (mi != mi) m = INFINITY;
+    }
+    m = finite_or_inf(m);
+  }
+#pragma unroll
+  for (int k = 16; k > 0; k >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, k));
+  if ((threadIdx.x & 31) == 0) atomicMax(&acc[c], (unsigned long long)__double_as_longlong(m));
+}
+
+// acc (bits of non-negative doubles) -> out, and acc back to zero for the next call
+__global__ void k_acc_drain(unsigned long long* __restrict__ acc, double* __restrict__ out, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  out[c] = __longlong_as_double((long long)acc[c]);
+  acc[c] = 0ull;
+}
+
 // ---------------------------------------------------------------- results
 // [group][bus][32] -> [case][bus]
 __global__ void k_gather_v(int nb, int ncases, const double2* V, double2* out) {

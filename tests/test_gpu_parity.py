@@ -166,3 +166,35 @@ def test_full_size_9241_bus_sample_matches_oracle(gpu):
     ref = _oracle(buses, branches, [cases[i] for i in idx], m.NR)
     sub = type(res)(res.v[idx], res.iterations[idx], res.status[idx], res.max_mis[idx])
     _compare(sub, ref)
+
+
+def test_mismatch_entry_point_matches_solve_and_oracle(gpu):
+    """mpf_mismatch at the solved voltages reproduces the solve's own final max |F|
+    and the oracle's mismatch at the same voltages."""
+    import torch
+
+    from mapol_b200._lib import lib
+
+    buses, branches, cases = m.workload("cfg1_300bus")
+    cases = cases[:40]
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.FP64)
+        res = pf.results()
+        v = torch.from_numpy(np.stack([res.v.real, res.v.imag], -1)).cuda()
+        out = torch.zeros(len(cases), dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            assert lib().mpf_mismatch(pf._h, v.data_ptr(), out.data_ptr(), None) == 0
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            np.testing.assert_allclose(got, res.max_mis, rtol=1e-6, atol=1e-15)
+        # an unconverged point: the flat start
+        flat = np.zeros((len(cases), len(buses)), complex)
+        flat[:] = buses["vm"] * np.exp(1j * buses["va"])
+        vf = torch.from_numpy(np.stack([flat.real, flat.imag], -1)).cuda()
+        assert lib().mpf_mismatch(pf._h, vf.data_ptr(), out.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+    for k in (0, 7, 31):
+        _, _, err = oracle.nr_system(buses, branches, flat[k], cases[k])
+        assert abs(got[k] - err) <= 1e-12 * max(1.0, err)
