@@ -194,6 +194,14 @@ int32_t mpf_runpf_host(mpf_handle* h, int32_t alg, int32_t precision,
                        double* v, int32_t* iterations, uint8_t* status,
                        double* max_mis);
 
+/* Max |F| of each case of the batch at the given voltages, F = [Re mis_pv; Re mis_pq;
+ * Im mis_pq] with each case's outages and injections: the batched counterpart of
+ * hybrid_checkConvergence (src/powerflow/newtonpf.h:526-568) and the max |F| loop
+ * that follows it (newtonpf.h:1241-1254).  v: device [n_cases][n_bus][2] (the
+ * layout of mpf_get_results_device); max_mis: device [n_cases].  Enqueued on
+ * stream; the first call allocates a small accumulator owned by the handle. */
+int32_t mpf_mismatch(mpf_handle* h, const double* v, double* max_mis, void* stream);
+
 /* Device time per kernel family of the last solve (synchronises the solve stream). */
 int32_t mpf_get_timing(mpf_handle* h, mpf_timing* t);
 
