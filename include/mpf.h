@@ -202,6 +202,19 @@ int32_t mpf_runpf_host(mpf_handle* h, int32_t alg, int32_t precision,
  * stream; the first call allocates a small accumulator owned by the handle. */
 int32_t mpf_mismatch(mpf_handle* h, const double* v, double* max_mis, void* stream);
 
+/* Same result as mpf_mismatch, for callers that must not allocate device memory at
+ * this point: code running inside CUDA stream capture, real-time loops that may not
+ * enter an allocator, or processes where another framework's memory pool owns the
+ * GPU.  No counterpart in the reference.  The call allocates nothing: its
+ * accumulator is a fixed 512 KB device array built into the library (held on every
+ * GPU that loads it until the process exits), so a batch may have at most 65536
+ * cases (MPF_ERR_BAD_INPUT beyond that).  The handle itself (mpf_create,
+ * mpf_set_cases) must have been set up beforehand.  The first call on each device
+ * looks up the array's device address; make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (different
+ * streams, or different handles on the same device) race and must be serialised. */
+int32_t mpf_mismatch_noalloc(mpf_handle* h, const double* v, double* max_mis, void* stream);
+
 /* Device time per kernel family of the last solve (synchronises the solve stream). */
 int32_t mpf_get_timing(mpf_handle* h, mpf_timing* t);
 

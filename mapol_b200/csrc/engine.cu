@@ -595,6 +595,34 @@ void solve_fd(mpf_handle* h, cudaStream_t st, int variant) {
 
 }  // namespace
 
+// ------------------------------------------------------------------ fixed-scratch mismatch
+// mpf_mismatch_noalloc keeps its per-case accumulator in this file-scope device array
+// instead of handle-owned memory, so the call never reaches an allocator.  The array
+// exists on every GPU that loads the library (512 KB each) until the process exits.
+// Host code may not use g_noalloc_acc as an address (it names a host-side shadow);
+// the device address comes from cudaGetSymbolAddress, once per device.
+constexpr int kNoAllocMaxCases = 65536;
+static __device__ __align__(256) unsigned long long g_noalloc_acc[kNoAllocMaxCases];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_acc on the current device (which must be `device`).
+cudaError_t noalloc_scratch(int device, unsigned long long** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_acc);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[device] = static_cast<unsigned long long*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+}  // namespace
+
 // ====================================================================== C-ABI
 extern "C" {
 
@@ -933,6 +961,32 @@ int32_t mpf_mismatch(mpf_handle* h, const double* v, double* max_mis, void* stre
     k_acc_drain<<<(h->ncases + 255) / 256, 256, 0, st>>>(h->eval_acc.as<unsigned long long>(), max_mis, h->ncases);
     CUDA_TRY(cudaGetLastError());
     h->last_stream = st;
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_mismatch_noalloc(mpf_handle* h, const double* v, double* max_mis, void* stream) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (!h->have_cases) return fail(h, MPF_ERR_STATE, "mpf_set_cases must be called before mpf_mismatch_noalloc");
+  if (!v || !max_mis) return fail(h, MPF_ERR_BAD_INPUT, "v and max_mis must be device pointers");
+  if (h->ncases > kNoAllocMaxCases)
+    return fail(h, MPF_ERR_BAD_INPUT,
+                "mpf_mismatch_noalloc handles at most " + std::to_string(kNoAllocMaxCases) + " cases per call (batch has " +
+                    std::to_string(h->ncases) + ")");
+  if (h->device < 0 || h->device >= kMaxDevices) return fail(h, MPF_ERR_BAD_INPUT, "device ordinal too large");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    unsigned long long* acc = nullptr;
+    CUDA_TRY(noalloc_scratch(h->device, &acc));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->own_stream;
+    // the array keeps whatever the previous call left: clear this call's slots
+    CUDA_TRY(cudaMemsetAsync(acc, 0, (size_t)h->ncases * sizeof(unsigned long long), st));
+    const int nfree = (int)h->g.mis_rows.size();
+    k_mismatch_eval<<<dim3((unsigned)((nfree + 255) / 256), (unsigned)h->ncases), 256, 0, st>>>(
+        h->dev(), reinterpret_cast<const double2*>(v), h->ncases, acc);
+    CUDA_TRY(cudaGetLastError());
+    k_acc_drain<<<(h->ncases + 255) / 256, 256, 0, st>>>(acc, max_mis, h->ncases);
+    CUDA_TRY(cudaGetLastError());
     return MPF_OK;
   });
 }
