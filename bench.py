@@ -183,10 +183,11 @@ def run_ours(args, rank, world, local_rank):
     from mapol_b200._lib import lib, ptr
     from mapol_b200.grid import cases_to_offsets
 
+    from mapol_b200.shard import max_over_ranks as _mor
+    from mapol_b200.shard import rank_cases
+
     torch.cuda.set_device(local_rank)
-    buses, branches, _ = m.workload(args.workload)
-    w = m.WORKLOADS[args.workload]
-    cases = m.n1_cases(branches, w["n_bus"], w["n_out"], 7 + rank, w["with_base"])
+    buses, branches, cases = rank_cases(args.workload, rank)
     n_cases = len(cases)
     pf = m.PowerFlow(buses, branches, device=local_rank)
     pf.set_cases(cases)
@@ -197,11 +198,7 @@ def run_ours(args, rank, world, local_rank):
             torch.distributed.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return _mor(x, world, "cuda")
 
     out = {}
     sampler = ClockSampler(local_rank) if rank == 0 else None
