@@ -75,7 +75,13 @@ void upload(DevBuf& b, const std::vector<T>& v) {
 
 // ------------------------------------------------------------------ LU system
 enum TaskClass { CLS_S = 0, CLS_M = 1, CLS_L = 2 };
-constexpr int kFmaxS = 8, kFmaxM = 24, kFmaxL = 83;
+// fronts up to kFmaxS: one case per thread; up to kFmaxM: a warp per 32-byte lane
+// chunk; larger: a 256-thread block per lane chunk, with fewer lanes per task when a
+// 32-byte chunk would not fit in shared memory (kSmemMax)
+constexpr int kFmaxS = 8, kFmaxM = 24;
+constexpr size_t kSmemMax = 227 * 1024;
+// largest front any task class can hold: one FP64 lane, f * ((f + 1) | 1) * 8 bytes
+constexpr int kFmaxAll = 167;
 
 struct Launch {
   int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
@@ -83,7 +89,7 @@ struct Launch {
 
 struct LUSystem {
   LUSymbolic sym;
-  DevBuf sn_c0, sn_f, sn_rptr, sn_rows, child_ptr, child_list, sn_parent, rel_ptr, relmap, ah_ptr, ah_loc;
+  DevBuf sn_w, sn_f, sn_rptr, sn_rows, child_ptr, child_list, sn_parent, rel_ptr, relmap, ah_ptr, ah_loc;
   DevBuf pan_off, cb_off, cbr_off, lev_sn;
   std::vector<Launch> factor_sched;  // ascending levels
   std::vector<Launch> level_sched;   // one launch per level (solves), ascending
@@ -100,7 +106,7 @@ struct LUSystem {
     d.nnz = sym.nnz;
     d.sumcb = sym.sum_cb;
     d.sumcbr = sym.cbr_off.empty() ? 0 : sym.cbr_off.back();
-    d.sn_c0 = sn_c0.as<int>();
+    d.sn_w = sn_w.as<int>();
     d.sn_f = sn_f.as<int>();
     d.sn_rptr = sn_rptr.as<int>();
     d.sn_rows = sn_rows.as<int>();
@@ -120,7 +126,7 @@ struct LUSystem {
   void setup(const LUSymbolic& s, const std::vector<int>& ahp, const std::vector<int>& ahl, int nA_) {
     sym = s;
     nA = nA_;
-    upload(sn_c0, s.sn_c0);
+    upload(sn_w, s.sn_w);
     upload(sn_f, s.sn_f);
     upload(sn_rptr, s.sn_rptr);
     upload(sn_rows, s.sn_rows);
@@ -201,7 +207,7 @@ struct Prec<float> { static constexpr int idx = 1; static constexpr int G = 8; }
 template <typename T, int G, int TEAM>
 void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x,
                        int* status, const int* group_active, int with_rhs, cudaStream_t st, int teams_per_block) {
-  const size_t team_elems = (size_t)ln.fcap * (ln.fcap + 1) * G;
+  const size_t team_elems = (size_t)ln.fcap * front_stride(ln.fcap) * G;
   const size_t smem = team_elems * sizeof(T) * teams_per_block;
   static bool attr_set = false;
   if (!attr_set) {
@@ -229,7 +235,15 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
     } else if (ln.cls == CLS_M) {
       launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 4);
     } else {
-      launch_factor_one<T, G, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+      const size_t per_lane = (size_t)ln.fcap * front_stride(ln.fcap) * sizeof(T);
+      if (per_lane * G <= kSmemMax)
+        launch_factor_one<T, G, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+      else if (per_lane * (G / 2) <= kSmemMax)
+        launch_factor_one<T, G / 2, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+      else if (per_lane * (G / 4) <= kSmemMax)
+        launch_factor_one<T, G / 4, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+      else
+        launch_factor_one<T, 1, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
     }
     ++*nlaunch;
   }
@@ -238,12 +252,18 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
 template <typename T>
 void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active, cudaStream_t st,
                    int* nlaunch) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set = true;
+  }
   for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
     const Launch& ln = sys.level_sched[k];
     const long long ntasks = (long long)ln.count * ngroups;
     long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-    k_mf_bsolve<T><<<(unsigned)blocks, 128, 0, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups,
-                                                     pan, x, group_active);
+    const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
+    k_mf_bsolve<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups,
+                                                        ln.fcap, pan, x, group_active);
     CUDA_TRY(cudaGetLastError());
     ++*nlaunch;
   }
@@ -378,7 +398,7 @@ struct mpf_handle {
     const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
     for (auto s : systems) {
       for (int p = 0; p < 2; ++p) b += s->A[p].bytes + s->pan[p].bytes + s->cb[p].bytes + s->cbr[p].bytes + s->x[p].bytes;
-      const DevBuf* idx[] = {&s->sn_c0, &s->sn_f, &s->sn_rptr, &s->sn_rows, &s->child_ptr, &s->child_list,
+      const DevBuf* idx[] = {&s->sn_w, &s->sn_f, &s->sn_rptr, &s->sn_rows, &s->child_ptr, &s->child_list,
                              &s->sn_parent, &s->rel_ptr, &s->relmap, &s->ah_ptr, &s->ah_loc, &s->pan_off,
                              &s->cb_off, &s->cbr_off, &s->lev_sn};
       for (auto q : idx) b += q->bytes;
@@ -681,10 +701,10 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
     const GridSymbolic& g = h->g;
     int maxf = g.jac.max_front;
     for (int v = 0; v < 2; ++v) maxf = std::max({maxf, g.bp[v].lu.max_front, g.bpp[v].lu.max_front});
-    if (maxf > kFmaxL)
+    if (maxf > kFmaxAll)
       return fail(h.get(), MPF_ERR_BAD_INPUT,
                   "largest frontal matrix (" + std::to_string(maxf) + ") exceeds the supported " +
-                      std::to_string(kFmaxL) + " (grid too densely meshed for shared-memory fronts)");
+                      std::to_string(kFmaxAll) + " (grid too densely meshed for shared-memory fronts)");
     CUDA_TRY(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaMallocHost(&h->h_any, sizeof(int)));
     CUDA_TRY(cudaEventCreate(&h->t0));

@@ -35,9 +35,10 @@ BranchY branch_admittance(double r, double x, double b, double tap, double shift
 // Multifrontal symbolic LU of a structurally symmetric n x n matrix factorised
 // without pivoting (diagonal pivots) in a fixed elimination order.
 //
-// Supernode s owns the consecutive pivot columns [sn_c0[s], sn_c0[s+1]) (w_s of
-// them) and its front rows R_s = sn_rows[sn_rptr[s] .. sn_rptr[s+1]) (f_s of them,
-// ascending, the first w_s are the pivots).  The front is the dense f x f matrix
+// Supernode s owns w_s pivot variables and its front rows R_s =
+// sn_rows[sn_rptr[s] .. sn_rptr[s+1]) (f_s of them, ascending; the first w_s are
+// the pivots, every other row is a later variable).  Pivots of an amalgamated
+// supernode need not be consecutive.  The front is the dense f x f matrix
 // A(R_s, R_s) restricted to the arrowhead of the pivots plus the contribution
 // blocks (CB) of the children; a partial LU of its first w pivots produces
 //   U-panel  F(0:w, 0:f)          w*f entries, row-major (holds L of the diagonal
@@ -52,7 +53,7 @@ struct LUSymbolic {
   int64_t nnz = 0;                   // entries of L+U (= sum of panel sizes)
   std::vector<int> etree_parent;     // per variable, -1 for roots
   int nsn = 0;
-  std::vector<int> sn_c0;            // nsn+1
+  std::vector<int> sn_w;             // pivots
   std::vector<int> sn_f;             // front size
   std::vector<int> sn_rptr, sn_rows; // front rows
   std::vector<int> sn_parent;        // -1 for roots
@@ -74,15 +75,26 @@ struct LUSymbolic {
   int64_t entry_pos(int row, int col) const;     // panel position of LU entry or -1
 };
 
+// Relaxed supernode amalgamation: a child joins its parent's front when the merged
+// front has at most max_pivots pivots and max_front rows and gains at most
+// max(max_zeros, max_zero_frac * size) explicit zeros.  max_pivots <= 1 disables it.
+struct Relax {
+  int max_pivots = 32;
+  int max_front = 83;
+  long long max_zeros = 16;
+  double max_zero_frac = 0.3;
+};
+
 // Builds the symbolic LU of the pattern given as symmetric adjacency (no diagonal)
 // in the already-permuted variable numbering.
-void lu_symbolic(int n, const std::vector<std::vector<int>>& adj, LUSymbolic& s);
+void lu_symbolic(int n, const std::vector<std::vector<int>>& adj, LUSymbolic& s, const Relax& relax = Relax());
 
 // Groups matrix entries (rows[e], cols[e]) by the supernode that owns min(row, col)
 // (its arrowhead).  a_index[e] = position of entry e in the grouped ("A-array")
 // order; supernode s owns A-array range [ah_ptr[s], ah_ptr[s+1]); ah_loc[k] is the
-// flat position row * (f + 1) + col of A-array entry k inside the front (the
-// front carries a right-hand-side column f).
+// flat position row * RS + col of A-array entry k inside the front, with the row
+// stride RS = (f + 1) | 1 (the front carries a right-hand-side column f; the odd
+// stride spreads consecutive rows over shared-memory banks).
 void arrowhead_layout(const LUSymbolic& s, const std::vector<int>& rows,
                       const std::vector<int>& cols, std::vector<int>& a_index,
                       std::vector<int>& ah_ptr, std::vector<int>& ah_loc);

@@ -64,7 +64,7 @@ struct DevGrid {
 struct DevLU {
   int n, nsn, nA;
   long long nnz, sumcb, sumcbr;
-  const int* sn_c0;
+  const int* sn_w;
   const int* sn_f;
   const int* sn_rptr;
   const int* sn_rows;
@@ -403,6 +403,10 @@ __device__ __forceinline__ void team_sync() {
   else __syncthreads();
 }
 
+// Row stride of a front in shared memory: f + 1 columns (right-hand side last),
+// rounded up to odd so that slots working on consecutive rows hit distinct banks.
+__host__ __device__ __forceinline__ int front_stride(int f) { return (f + 1) | 1; }
+
 template <typename T, int G, int TEAM>
 __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
     DevLU L, const int* __restrict__ task_sn, int nsn_l, int ngroups, int fcap,
@@ -414,7 +418,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
   const int teams = blockDim.x / TEAM;
   const int team = threadIdx.x / TEAM, tid = threadIdx.x % TEAM;
   const int slot = tid / G, l = tid % G;
-  T* F = reinterpret_cast<T*>(smem_raw) + (size_t)team * fcap * (fcap + 1) * G;
+  T* F = reinterpret_cast<T*>(smem_raw) + (size_t)team * fcap * front_stride(fcap) * G;
   const long long nchunks = (long long)ngroups * LPG;
   const long long ntasks = (long long)nsn_l * nchunks;
   for (long long t = (long long)blockIdx.x * teams + team; t < ntasks; t += (long long)gridDim.x * teams) {
@@ -423,68 +427,68 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
     const int g = ch / LPG;
     if (!group_active[g]) continue;
     const int lane = (ch % LPG) * G + l;
-    const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s];
-    const int f1 = f + 1;
-    for (int idx = slot; idx < f * f1; idx += SLOTS) F[idx * G + l] = (T)0;
+    const int w = L.sn_w[s], f = L.sn_f[s];
+    const int* rows = L.sn_rows + L.sn_rptr[s];
+    const int RS = front_stride(f);
+    const int ncols = with_rhs ? f + 1 : f;
+#define FR(r, c) F[((r) * RS + (c)) * G + l]
+    for (int idx = slot; idx < f * RS; idx += SLOTS) F[idx * G + l] = (T)0;
     team_sync<TEAM>();
-    for (int e = L.ah_ptr[s] + slot; e < L.ah_ptr[s + 1]; e += SLOTS)
-      F[L.ah_loc[e] * G + l] = A[at32(g, L.nA, e, lane)];
+    for (int e = L.ah_ptr[s] + slot; e < L.ah_ptr[s + 1]; e += SLOTS) F[L.ah_loc[e] * G + l] = A[at32(g, L.nA, e, lane)];
     if (with_rhs)
-      for (int p = slot; p < w; p += SLOTS) F[(p * f1 + f) * G + l] = x[at32(g, L.n, c0 + p, lane)];
+      for (int p = slot; p < w; p += SLOTS) FR(p, f) = x[at32(g, L.n, rows[p], lane)];
     team_sync<TEAM>();
     for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
       const int ch2 = L.child_list[ci];
-      const int m = L.sn_f[ch2] - (L.sn_c0[ch2 + 1] - L.sn_c0[ch2]);
+      const int m = L.sn_f[ch2] - L.sn_w[ch2];
       const int* rel = L.relmap + L.rel_ptr[ch2];
       const long long cbo = L.cb_off[ch2];
-      for (int idx = slot; idx < m * m; idx += SLOTS) {
-        const int a = idx / m, b = idx - a * m;
-        F[(rel[a] * f1 + rel[b]) * G + l] += cb[at32(g, L.sumcb, cbo + idx, lane)];
+      for (int a = slot; a < m; a += SLOTS) {
+        const int ra = rel[a];
+        const T* src = cb + at32(g, L.sumcb, cbo + (long long)a * m, lane);
+        for (int b = 0; b < m; ++b) FR(ra, rel[b]) += src[(size_t)b * 32];
+        if (with_rhs) FR(ra, f) += cbr[at32(g, L.sumcbr, L.cbr_off[ch2] + a, lane)];
       }
-      if (with_rhs)
-        for (int a = slot; a < m; a += SLOTS)
-          F[(rel[a] * f1 + f) * G + l] += cbr[at32(g, L.sumcbr, L.cbr_off[ch2] + a, lane)];
       team_sync<TEAM>();
     }
-    const int ncol_extra = with_rhs ? 1 : 0;
     for (int p = 0; p < w; ++p) {
-      T piv = F[(p * f1 + p) * G + l];
+      T piv = FR(p, p);
       if (!(fabs((double)piv) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)piv) <= DBL_MAX)) {
         if (slot == 0) status[g * 32 + lane] = ST_SINGULAR;
         piv = (T)1;
       }
       const T inv = (T)1 / piv;
-      for (int i = p + 1 + slot; i < f; i += SLOTS) F[(i * f1 + p) * G + l] *= inv;
-      team_sync<TEAM>();
-      const int nrow = f - p - 1, ncol = f - p - 1 + ncol_extra;
-      for (int idx = slot; idx < nrow * ncol; idx += SLOTS) {
-        const int i = p + 1 + idx / ncol, q = p + 1 + idx % ncol;
-        F[(i * f1 + q) * G + l] -= F[(i * f1 + p) * G + l] * F[(p * f1 + q) * G + l];
+      // each slot owns rows i = p+1+slot, p+1+slot+SLOTS, ...: scale L(i,p), then
+      // update row i with the (broadcast) pivot row
+      for (int i = p + 1 + slot; i < f; i += SLOTS) {
+        const T lip = FR(i, p) * inv;
+        FR(i, p) = lip;
+        for (int q = p + 1; q < ncols; ++q) FR(i, q) -= lip * FR(p, q);
       }
       team_sync<TEAM>();
     }
     const long long po = L.pan_off[s];
-    for (int idx = slot; idx < w * f; idx += SLOTS) {
-      const int p = idx / f, q = idx - p * f;
-      pan[at32(g, L.nnz, po + idx, lane)] = F[(p * f1 + q) * G + l];
+    // U-panel: rows 0..w-1, all f columns; L-panel: rows w..f-1, columns 0..w-1
+    for (int p = slot; p < w; p += SLOTS) {
+      T* dst = pan + at32(g, L.nnz, po + (long long)p * f, lane);
+      for (int q = 0; q < f; ++q) dst[(size_t)q * 32] = FR(p, q);
     }
     const int m = f - w;
-    for (int idx = slot; idx < m * w; idx += SLOTS) {
-      const int i = w + idx / w, q = idx % w;
-      pan[at32(g, L.nnz, po + (long long)w * f + idx, lane)] = F[(i * f1 + q) * G + l];
+    for (int i = slot; i < m; i += SLOTS) {
+      T* dst = pan + at32(g, L.nnz, po + (long long)w * f + (long long)i * w, lane);
+      for (int q = 0; q < w; ++q) dst[(size_t)q * 32] = FR(w + i, q);
     }
     if (with_rhs)
-      for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, c0 + p, lane)] = F[(p * f1 + f) * G + l];
+      for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, rows[p], lane)] = FR(p, f);
     if (L.sn_parent[s] >= 0) {
       const long long cbo = L.cb_off[s];
-      for (int idx = slot; idx < m * m; idx += SLOTS) {
-        const int a = idx / m, b = idx - a * m;
-        cb[at32(g, L.sumcb, cbo + idx, lane)] = F[((w + a) * f1 + w + b) * G + l];
+      for (int a = slot; a < m; a += SLOTS) {
+        T* dst = cb + at32(g, L.sumcb, cbo + (long long)a * m, lane);
+        for (int b = 0; b < m; ++b) dst[(size_t)b * 32] = FR(w + a, w + b);
+        if (with_rhs) cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = FR(w + a, f);
       }
-      if (with_rhs)
-        for (int a = slot; a < m; a += SLOTS)
-          cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = F[((w + a) * f1 + f) * G + l];
     }
+#undef FR
     team_sync<TEAM>();
   }
 }
@@ -504,12 +508,13 @@ __global__ void __launch_bounds__(128) k_mf_fsolve(DevLU L, const int* __restric
     const int s = task_sn[t / ngroups];
     const int g = (int)(t % ngroups);
     if (!group_active[g]) continue;
-    const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s];
+    const int w = L.sn_w[s], f = L.sn_f[s];
+    const int* rows = L.sn_rows + L.sn_rptr[s];
     for (int i = 0; i < f; ++i) b[i * 32 + lane] = (T)0;
-    for (int p = 0; p < w; ++p) b[p * 32 + lane] = x[at32(g, L.n, c0 + p, lane)];
+    for (int p = 0; p < w; ++p) b[p * 32 + lane] = x[at32(g, L.n, rows[p], lane)];
     for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
       const int ch = L.child_list[ci];
-      const int m = L.sn_f[ch] - (L.sn_c0[ch + 1] - L.sn_c0[ch]);
+      const int m = L.sn_f[ch] - L.sn_w[ch];
       const int* rel = L.relmap + L.rel_ptr[ch];
       for (int a = 0; a < m; ++a) b[rel[a] * 32 + lane] += cbr[at32(g, L.sumcbr, L.cbr_off[ch] + a, lane)];
     }
@@ -520,35 +525,48 @@ __global__ void __launch_bounds__(128) k_mf_fsolve(DevLU L, const int* __restric
       for (int i = w; i < f; ++i)
         b[i * 32 + lane] -= pan[at32(g, L.nnz, po + (long long)w * f + (long long)(i - w) * w + p, lane)] * yp;
     }
-    for (int p = 0; p < w; ++p) x[at32(g, L.n, c0 + p, lane)] = b[p * 32 + lane];
+    for (int p = 0; p < w; ++p) x[at32(g, L.n, rows[p], lane)] = b[p * 32 + lane];
     if (L.sn_parent[s] >= 0)
       for (int a = 0; a < f - w; ++a) cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = b[(w + a) * 32 + lane];
     __syncwarp();
   }
 }
 
-// Backward substitution: thread per case, warp per (supernode, group); ancestors'
-// solutions are final (previous launches), the pivots' own are solved in order.
+// Backward substitution: thread per case, warp per (supernode, group).  The
+// supernode's front values of x (ancestors' solutions, final after the previous
+// launches, and its own forward-substituted y) are staged in shared memory first,
+// so the dependent chain over the w pivots runs on shared memory while the
+// U-panel rows stream from global memory.
 template <typename T>
 __global__ void __launch_bounds__(128) k_mf_bsolve(DevLU L, const int* __restrict__ task_sn, int nsn_l,
-                                                   int ngroups, const T* __restrict__ pan, T* __restrict__ x,
-                                                   const int* __restrict__ group_active) {
+                                                   int ngroups, int fcap, const T* __restrict__ pan,
+                                                   T* __restrict__ x, const int* __restrict__ group_active) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  T* xs = reinterpret_cast<T*>(smem_raw) + (size_t)warp * fcap * 32;
   const long long ntasks = (long long)nsn_l * ngroups;
   for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
     const int s = task_sn[t / ngroups];
     const int g = (int)(t % ngroups);
     if (!group_active[g]) continue;
-    const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s];
+    const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     const long long po = L.pan_off[s];
+    for (int q = 0; q < f; ++q) xs[q * 32 + lane] = x[at32(g, L.n, rows[q], lane)];
     for (int p = w - 1; p >= 0; --p) {
-      T acc = x[at32(g, L.n, c0 + p, lane)];
-      const T* urow = pan;  // U-panel row p: entries (p, q), q = 0..f-1
-      for (int q = p + 1; q < f; ++q)
-        acc -= urow[at32(g, L.nnz, po + (long long)p * f + q, lane)] * x[at32(g, L.n, rows[q], lane)];
-      x[at32(g, L.n, c0 + p, lane)] = acc / urow[at32(g, L.nnz, po + (long long)p * f + p, lane)];
+      const T* urow = pan + at32(g, L.nnz, po + (long long)p * f, lane);
+      T acc = xs[p * 32 + lane];
+      T acc2 = (T)0;
+      int q = p + 1;
+      for (; q + 1 < f; q += 2) {
+        acc -= urow[(size_t)q * 32] * xs[q * 32 + lane];
+        acc2 -= urow[(size_t)(q + 1) * 32] * xs[(q + 1) * 32 + lane];
+      }
+      if (q < f) acc -= urow[(size_t)q * 32] * xs[q * 32 + lane];
+      xs[p * 32 + lane] = (acc + acc2) / urow[(size_t)p * 32];
     }
+    for (int p = 0; p < w; ++p) x[at32(g, L.n, rows[p], lane)] = xs[p * 32 + lane];
+    __syncwarp();
   }
 }
 

@@ -92,13 +92,13 @@ int64_t LUSymbolic::entry_pos(int row, int col) const {
   const int s = sn_of[std::min(row, col)];
   const int lr = local(s, row), lc = local(s, col);
   if (lr < 0 || lc < 0) return -1;
-  const int w = sn_c0[s + 1] - sn_c0[s], f = sn_f[s];
+  const int w = sn_w[s], f = sn_f[s];
   if (lr < w) return pan_off[s] + (int64_t)lr * f + lc;
   if (lc < w) return pan_off[s] + (int64_t)w * f + (int64_t)(lr - w) * w + lc;
   return -1;
 }
 
-void lu_symbolic(int n, const std::vector<std::vector<int>>& adj, LUSymbolic& s) {
+void lu_symbolic(int n, const std::vector<std::vector<int>>& adj, LUSymbolic& s, const Relax& relax) {
   s = LUSymbolic();
   s.n = n;
   // elimination tree (Liu), using the entries left of the diagonal of each row
@@ -137,31 +137,94 @@ void lu_symbolic(int n, const std::vector<std::vector<int>>& adj, LUSymbolic& s)
   }
   // fundamental supernodes: j joins j-1 when j is j-1's parent, its only child,
   // and L(:,j) = L(:,j-1) minus row j
-  s.sn_c0.clear();
+  std::vector<int> fs_c0;
   for (int j = 0; j < n; ++j) {
     const bool join = j > 0 && parent[j - 1] == j && children[j].size() == 1 &&
                       Ls[j].size() + 1 == Ls[j - 1].size();
-    if (!join) s.sn_c0.push_back(j);
+    if (!join) fs_c0.push_back(j);
   }
-  s.nsn = (int)s.sn_c0.size();
-  s.sn_c0.push_back(n);
-  const int ns = s.nsn;
+  const int nfs = (int)fs_c0.size();
+  fs_c0.push_back(n);
+  std::vector<int> fs_of(n);
+  for (int q = 0; q < nfs; ++q)
+    for (int j = fs_c0[q]; j < fs_c0[q + 1]; ++j) fs_of[j] = q;
+  std::vector<int> fs_parent(nfs, -1);
+  std::vector<std::vector<int>> fs_children(nfs);
+  for (int q = 0; q < nfs; ++q) {
+    const int last = fs_c0[q + 1] - 1;
+    if (parent[last] >= 0) {
+      fs_parent[q] = fs_of[parent[last]];
+      fs_children[fs_parent[q]].push_back(q);
+    }
+  }
+  // Relaxed amalgamation: merge a child supernode into its parent when the merged
+  // front stays small and gains few explicit zeros.  The child's pivots join the
+  // parent's front (all its contribution-block rows are already there), so its
+  // contribution block never leaves the front.  Merged pivot sets need not be
+  // consecutive; siblings' pivots are independent.  Children have lower indices
+  // than parents, so one increasing pass sees every child before its parent.
+  std::vector<int> grp(nfs);                  // group representative (a parent-most supernode)
+  std::vector<int> gw(nfs), gf(nfs);          // pivots and front size of the group rooted here
+  std::vector<long long> gnnz(nfs);           // true panel entries of the group
+  for (int q = 0; q < nfs; ++q) {
+    grp[q] = q;
+    gw[q] = fs_c0[q + 1] - fs_c0[q];
+    gf[q] = 1 + (int)Ls[fs_c0[q]].size();
+    gnnz[q] = 2LL * gw[q] * gf[q] - (long long)gw[q] * gw[q];
+  }
+  if (relax.max_pivots > 1) {
+    for (int q = 0; q < nfs; ++q) {
+      std::vector<int> ch = fs_children[q];
+      std::sort(ch.begin(), ch.end(), [&](int a, int b) { return gw[a] < gw[b] || (gw[a] == gw[b] && a < b); });
+      for (int c : ch) {
+        const int wm = gw[q] + gw[c], fm = gf[q] + gw[c];
+        if (wm > relax.max_pivots || fm > relax.max_front) continue;
+        const long long size = 2LL * wm * fm - (long long)wm * wm;
+        const long long zeros = size - (gnnz[q] + gnnz[c]);
+        if (zeros > relax.max_zeros && (double)zeros > relax.max_zero_frac * (double)size) continue;
+        grp[c] = q;
+        gw[q] = wm;
+        gf[q] = fm;
+        gnnz[q] += gnnz[c];
+      }
+    }
+  }
+  // resolve groups to their final representative (a merged child's own children
+  // that merged into it are already pointing at it)
+  std::vector<int> rep(nfs);
+  for (int q = nfs - 1; q >= 0; --q) rep[q] = (grp[q] == q) ? q : rep[grp[q]];
+  std::vector<int> final_id(nfs, -1);
+  int ns = 0;
+  for (int q = 0; q < nfs; ++q)
+    if (rep[q] == q) final_id[q] = ns++;
+  s.nsn = ns;
+  s.sn_w.assign(ns, 0);
+  s.sn_f.assign(ns, 0);
   s.sn_of.assign(n, -1);
-  s.sn_f.resize(ns);
-  s.sn_rptr.assign(ns + 1, 0);
-  for (int q = 0; q < ns; ++q) {
-    const int c0 = s.sn_c0[q];
-    for (int j = c0; j < s.sn_c0[q + 1]; ++j) s.sn_of[j] = q;
-    s.sn_f[q] = 1 + (int)Ls[c0].size();
-    s.sn_rptr[q + 1] = s.sn_rptr[q] + s.sn_f[q];
-    s.sn_rows.push_back(c0);
-    s.sn_rows.insert(s.sn_rows.end(), Ls[c0].begin(), Ls[c0].end());
-    s.max_front = std::max(s.max_front, s.sn_f[q]);
+  std::vector<std::vector<int>> piv(ns);
+  for (int q = 0; q < nfs; ++q) {
+    const int t = final_id[rep[q]];
+    for (int j = fs_c0[q]; j < fs_c0[q + 1]; ++j) {
+      piv[t].push_back(j);
+      s.sn_of[j] = t;
+    }
   }
+  s.sn_rptr.assign(ns + 1, 0);
   s.sn_parent.assign(ns, -1);
-  for (int q = 0; q < ns; ++q) {
-    const int last = s.sn_c0[q + 1] - 1;
-    if (parent[last] >= 0) s.sn_parent[q] = s.sn_of[parent[last]];
+  for (int q = 0; q < nfs; ++q) {
+    if (rep[q] != q) continue;
+    const int t = final_id[q];
+    std::vector<int>& pv = piv[t];
+    std::sort(pv.begin(), pv.end());
+    const int last = fs_c0[q + 1] - 1;  // the representative's last pivot: its L rows form the CB
+    std::vector<int> rows(pv);
+    for (int i : Ls[last]) rows.push_back(i);
+    s.sn_w[t] = (int)pv.size();
+    s.sn_f[t] = (int)rows.size();
+    s.sn_rptr[t + 1] = s.sn_rptr[t] + s.sn_f[t];
+    s.sn_rows.insert(s.sn_rows.end(), rows.begin(), rows.end());
+    s.max_front = std::max(s.max_front, s.sn_f[t]);
+    if (parent[last] >= 0) s.sn_parent[t] = s.sn_of[parent[last]];
   }
   // children lists, levels
   s.child_ptr.assign(ns + 1, 0);
@@ -194,13 +257,13 @@ void lu_symbolic(int n, const std::vector<std::vector<int>>& adj, LUSymbolic& s)
       std::stable_sort(s.lev_sn.begin() + s.lev_ptr[l], s.lev_sn.begin() + s.lev_ptr[l + 1],
                        [&](int a, int b) { return s.sn_f[a] < s.sn_f[b]; });
   }
-  // storage offsets, relative maps, flops
+  // storage offsets, relative maps, flops (of the dense fronts, explicit zeros included)
   s.pan_off.assign(ns + 1, 0);
   s.cb_off.assign(ns + 1, 0);
   s.cbr_off.assign(ns + 1, 0);
   s.rel_ptr.assign(ns + 1, 0);
   for (int q = 0; q < ns; ++q) {
-    const int w = s.sn_c0[q + 1] - s.sn_c0[q], f = s.sn_f[q];
+    const int w = s.sn_w[q], f = s.sn_f[q];
     s.pan_off[q + 1] = s.pan_off[q] + (int64_t)w * f + (int64_t)(f - w) * w;
     s.cb_off[q + 1] = s.cb_off[q] + (int64_t)(f - w) * (f - w);
     s.cbr_off[q + 1] = s.cbr_off[q] + (f - w);
@@ -217,11 +280,10 @@ void lu_symbolic(int n, const std::vector<std::vector<int>>& adj, LUSymbolic& s)
   for (int q = 0; q < ns; ++q) {
     const int par = s.sn_parent[q];
     if (par < 0) continue;
-    const int w = s.sn_c0[q + 1] - s.sn_c0[q], f = s.sn_f[q];
+    const int w = s.sn_w[q], f = s.sn_f[q];
     for (int t = 0; t < f - w; ++t) {
       const int var = s.sn_rows[s.sn_rptr[q] + w + t];
-      const int li = s.local(par, var);
-      s.relmap[s.rel_ptr[q] + t] = li;  // always >= 0 (CB rows are in the parent's front)
+      s.relmap[s.rel_ptr[q] + t] = s.local(par, var);  // always >= 0 (CB rows are in the parent's front)
     }
   }
 }
@@ -245,7 +307,7 @@ void arrowhead_layout(const LUSymbolic& s, const std::vector<int>& rows,
     const int k = fill[q]++;
     a_index[e] = k;
     const int f = s.sn_f[q];
-    ah_loc[k] = s.local(q, rows[e]) * (f + 1) + s.local(q, cols[e]);
+    ah_loc[k] = s.local(q, rows[e]) * ((f + 1) | 1) + s.local(q, cols[e]);
   }
 }
 

@@ -34,14 +34,15 @@ static double solve_check(const LUSymbolic& L, const std::vector<int>& ah_ptr, c
   for (int lv = 0; lv < L.nlevels; ++lv) {
     for (int k = L.lev_ptr[lv]; k < L.lev_ptr[lv + 1]; ++k) {
       const int s = L.lev_sn[k];
-      const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s], f1 = f + 1;
-      std::vector<double> F((size_t)f * f1, 0.0);
+      const int w = L.sn_w[s], f = L.sn_f[s], f1 = (f + 1) | 1;
+      const int* rw = L.sn_rows.data() + L.sn_rptr[s];
+      std::vector<double> F((size_t)f * f1, 0.0);  // row stride (f + 1) | 1 as in the kernel
       for (int e = ah_ptr[s]; e < ah_ptr[s + 1]; ++e) F[ah_loc[e]] = A[e];
       if (fused_forward)
-        for (int p = 0; p < w; ++p) F[p * f1 + f] = x[c0 + p];
+        for (int p = 0; p < w; ++p) F[p * f1 + f] = x[rw[p]];
       for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
         const int ch = L.child_list[ci];
-        const int mm = L.sn_f[ch] - (L.sn_c0[ch + 1] - L.sn_c0[ch]);
+        const int mm = L.sn_f[ch] - L.sn_w[ch];
         const int* rel = L.relmap.data() + L.rel_ptr[ch];
         for (int idx = 0; idx < mm * mm; ++idx) F[rel[idx / mm] * f1 + rel[idx % mm]] += cb[L.cb_off[ch] + idx];
         if (fused_forward)
@@ -58,7 +59,7 @@ static double solve_check(const LUSymbolic& L, const std::vector<int>& ah_ptr, c
       const int mm = f - w;
       for (int idx = 0; idx < mm * w; ++idx) pan[L.pan_off[s] + (long)w * f + idx] = F[(w + idx / w) * f1 + idx % w];
       if (fused_forward)
-        for (int p = 0; p < w; ++p) x[c0 + p] = F[p * f1 + f];
+        for (int p = 0; p < w; ++p) x[rw[p]] = F[p * f1 + f];
       if (L.sn_parent[s] >= 0) {
         for (int idx = 0; idx < mm * mm; ++idx) cb[L.cb_off[s] + idx] = F[(w + idx / mm) * f1 + w + idx % mm];
         if (fused_forward)
@@ -70,12 +71,13 @@ static double solve_check(const LUSymbolic& L, const std::vector<int>& ah_ptr, c
     for (int lv = 0; lv < L.nlevels; ++lv)
       for (int k = L.lev_ptr[lv]; k < L.lev_ptr[lv + 1]; ++k) {
         const int s = L.lev_sn[k];
-        const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s];
+        const int w = L.sn_w[s], f = L.sn_f[s];
+        const int* rw = L.sn_rows.data() + L.sn_rptr[s];
         std::vector<double> bl(f, 0.0);
-        for (int p = 0; p < w; ++p) bl[p] = x[c0 + p];
+        for (int p = 0; p < w; ++p) bl[p] = x[rw[p]];
         for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
           const int ch = L.child_list[ci];
-          const int mm = L.sn_f[ch] - (L.sn_c0[ch + 1] - L.sn_c0[ch]);
+          const int mm = L.sn_f[ch] - L.sn_w[ch];
           const int* rel = L.relmap.data() + L.rel_ptr[ch];
           for (int a = 0; a < mm; ++a) bl[rel[a]] += cbr[L.cbr_off[ch] + a];
         }
@@ -83,7 +85,7 @@ static double solve_check(const LUSymbolic& L, const std::vector<int>& ah_ptr, c
           for (int i = p + 1; i < w; ++i) bl[i] -= pan[L.pan_off[s] + (long)i * f + p] * bl[p];
           for (int i = w; i < f; ++i) bl[i] -= pan[L.pan_off[s] + (long)w * f + (long)(i - w) * w + p] * bl[p];
         }
-        for (int p = 0; p < w; ++p) x[c0 + p] = bl[p];
+        for (int p = 0; p < w; ++p) x[rw[p]] = bl[p];
         if (L.sn_parent[s] >= 0)
           for (int a = 0; a < f - w; ++a) cbr[L.cbr_off[s] + a] = bl[w + a];
       }
@@ -92,12 +94,12 @@ static double solve_check(const LUSymbolic& L, const std::vector<int>& ah_ptr, c
   for (int lv = L.nlevels - 1; lv >= 0; --lv)
     for (int k = L.lev_ptr[lv]; k < L.lev_ptr[lv + 1]; ++k) {
       const int s = L.lev_sn[k];
-      const int c0 = L.sn_c0[s], w = L.sn_c0[s + 1] - c0, f = L.sn_f[s];
+      const int w = L.sn_w[s], f = L.sn_f[s];
       const int* rw = L.sn_rows.data() + L.sn_rptr[s];
       for (int p = w - 1; p >= 0; --p) {
-        double acc = x[c0 + p];
+        double acc = x[rw[p]];
         for (int q = p + 1; q < f; ++q) acc -= pan[L.pan_off[s] + (long)p * f + q] * x[rw[q]];
-        x[c0 + p] = acc / pan[L.pan_off[s] + (long)p * f + p];
+        x[rw[p]] = acc / pan[L.pan_off[s] + (long)p * f + p];
       }
     }
   // residual check against the matrix: r = A x - b
@@ -153,7 +155,7 @@ int main(int argc, char** argv) {
       r2.resize(fs.base.size());
       c2.resize(fs.base.size());
       for (int s = 0; s < fs.lu.nsn; ++s) {
-        const int f1 = fs.lu.sn_f[s] + 1;
+        const int f1 = (fs.lu.sn_f[s] + 1) | 1;
         const int* rw = fs.lu.sn_rows.data() + fs.lu.sn_rptr[s];
         for (int e = fs.ah_ptr[s]; e < fs.ah_ptr[s + 1]; ++e) {
           r2[e] = rw[fs.ah_loc[e] / f1];
