@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cases", type=int, default=0,
+                    help="solve only the first N cases per GPU (small runs for profiling; 0 = all)")
     return ap.parse_args()
 
 
@@ -188,6 +190,8 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     buses, branches, cases = rank_cases(args.workload, rank)
+    if args.cases:
+        cases = cases[: args.cases]
     n_cases = len(cases)
     pf = m.PowerFlow(buses, branches, device=local_rank)
     pf.set_cases(cases)

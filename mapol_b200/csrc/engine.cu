@@ -74,11 +74,11 @@ void upload(DevBuf& b, const std::vector<T>& v) {
 }
 
 // ------------------------------------------------------------------ LU system
-enum TaskClass { CLS_S = 0, CLS_M = 1, CLS_L = 2 };
+enum TaskClass { CLS_S = 0, CLS_M = 1, CLS_L = 2, CLS_M1 = 3 };
 // fronts up to kFmaxS: one case per thread; up to kFmaxM: a warp per 32-byte lane
 // chunk; larger: a 256-thread block per lane chunk, with fewer lanes per task when a
 // 32-byte chunk would not fit in shared memory (kSmemMax)
-constexpr int kFmaxS = 8, kFmaxM = 24;
+constexpr int kFmaxS = 8, kFmaxM1 = 16, kFmaxM = 24;
 constexpr size_t kSmemMax = 227 * 1024;
 // largest front any task class can hold: one FP64 lane, f * ((f + 1) | 1) * 8 bytes
 constexpr int kFmaxAll = 167;
@@ -152,12 +152,14 @@ struct LUSystem {
       level_sched.push_back({b, e - b, 0, fmax_all});
       int k = b;
       while (k < e) {
-        const int f0 = s.sn_f[s.lev_sn[k]];
-        const int cls = f0 <= kFmaxS ? CLS_S : (f0 <= kFmaxM ? CLS_M : CLS_L);
+        auto cls_of = [](int f) {
+          return f <= kFmaxS ? CLS_S : f <= kFmaxM1 ? CLS_M1 : f <= kFmaxM ? CLS_M : CLS_L;
+        };
+        const int cls = cls_of(s.sn_f[s.lev_sn[k]]);
         int k2 = k, fcap = 0;
         while (k2 < e) {
           const int f = s.sn_f[s.lev_sn[k2]];
-          const int c2 = f <= kFmaxS ? CLS_S : (f <= kFmaxM ? CLS_M : CLS_L);
+          const int c2 = cls_of(f);
           if (c2 != cls) break;
           fcap = std::max(fcap, f);
           ++k2;
@@ -232,6 +234,8 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
       // one case per thread, fronts up to 8 x 9
       const int tpb = sizeof(T) == 8 ? 4 : 8;
       launch_factor_one<T, 32, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, tpb);
+    } else if (ln.cls == CLS_M1) {
+      launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 8);
     } else if (ln.cls == CLS_M) {
       launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 4);
     } else {
@@ -252,18 +256,29 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
 template <typename T>
 void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active, cudaStream_t st,
                    int* nlaunch) {
+  constexpr int G = Prec<T>::G;
   static bool attr_set = false;
   if (!attr_set) {
     CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     attr_set = true;
   }
   for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
     const Launch& ln = sys.level_sched[k];
-    const long long ntasks = (long long)ln.count * ngroups;
-    long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-    const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
-    k_mf_bsolve<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups,
-                                                        ln.fcap, pan, x, group_active);
+    if (ln.fcap <= kFmaxM1) {
+      // small fronts: one case per thread
+      const long long ntasks = (long long)ln.count * ngroups;
+      const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
+      const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
+      k_mf_bsolve<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
+                                                          ngroups, ln.fcap, pan, x, group_active);
+    } else {
+      const long long ntasks = (long long)ln.count * ngroups * (32 / G);
+      const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
+      const size_t smem = (size_t)4 * ln.fcap * G * sizeof(T);
+      k_mf_bsolve_chunk<T, G><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset,
+                                                                   ln.count, ngroups, ln.fcap, pan, x, group_active);
+    }
     CUDA_TRY(cudaGetLastError());
     ++*nlaunch;
   }

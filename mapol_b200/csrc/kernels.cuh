@@ -570,6 +570,46 @@ __global__ void __launch_bounds__(128) k_mf_bsolve(DevLU L, const int* __restric
   }
 }
 
+// Backward substitution for large fronts: warp per (supernode, chunk of G lanes);
+// SLOTS = 32 / G threads per lane split each pivot row's dot product and fold it
+// with shuffles, so a big supernode's chain of w pivots runs on 8x (FP64) or 4x
+// (FP32) more warps than the thread-per-case kernel.
+template <typename T, int G>
+__global__ void __launch_bounds__(128) k_mf_bsolve_chunk(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+                                                         int ngroups, int fcap, const T* __restrict__ pan,
+                                                         T* __restrict__ x, const int* __restrict__ group_active) {
+  constexpr int SLOTS = 32 / G, LPG = 32 / G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  const int slot = tid / G, l = tid % G;
+  T* xs = reinterpret_cast<T*>(smem_raw) + (size_t)warp * fcap * G;
+  const long long nchunks = (long long)ngroups * LPG;
+  const long long ntasks = (long long)nsn_l * nchunks;
+  for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
+    const int s = task_sn[t / nchunks];
+    const int ch = (int)(t % nchunks);
+    const int g = ch / LPG;
+    if (!group_active[g]) continue;
+    const int lane = (ch % LPG) * G + l;
+    const int w = L.sn_w[s], f = L.sn_f[s];
+    const int* rows = L.sn_rows + L.sn_rptr[s];
+    const long long po = L.pan_off[s];
+    for (int q = slot; q < f; q += SLOTS) xs[q * G + l] = x[at32(g, L.n, rows[q], lane)];
+    __syncwarp();
+    for (int p = w - 1; p >= 0; --p) {
+      const T* urow = pan + at32(g, L.nnz, po + (long long)p * f, lane);
+      T part = (T)0;
+      for (int q = p + 1 + slot; q < f; q += SLOTS) part += urow[(size_t)q * 32] * xs[q * G + l];
+#pragma unroll
+      for (int o = 16; o >= G; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if (slot == 0) xs[p * G + l] = (xs[p * G + l] - part) / urow[(size_t)p * 32];
+      __syncwarp();
+    }
+    for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, rows[p], lane)] = xs[p * G + l];
+    __syncwarp();
+  }
+}
+
 // ---------------------------------------------------------------- mismatch of given voltages
 // max |F| per case for voltages given case-major (v[c][i], the layout results use),
 // F = [Re mis_pv; Re mis_pq; Im mis_pq] as newtonpf.h:18-71 (hybrid_checkConvergence,
