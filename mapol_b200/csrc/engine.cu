@@ -225,12 +225,21 @@ void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const
   CUDA_TRY(cudaGetLastError());
 }
 
+// Warp teams need enough tasks to fill the GPU; a launch with fewer tasks gives
+// each front a 256-thread team instead (8x the threads on the same chain of pivots).
+constexpr long long kMinWarpTasks = 148LL * 24;
+
 template <typename T>
 void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x, int* status,
                    const int* group_active, int with_rhs, cudaStream_t st, int* nlaunch) {
   constexpr int G = Prec<T>::G;
   for (const Launch& ln : sys.factor_sched) {
-    if (ln.cls == CLS_S) {
+    const long long lanes_tasks = (long long)ln.count * ngroups;
+    if (ln.cls == CLS_S && lanes_tasks < kMinWarpTasks) {
+      launch_factor_one<T, 32, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+    } else if ((ln.cls == CLS_M1 || ln.cls == CLS_M) && lanes_tasks * (32 / G) < kMinWarpTasks) {
+      launch_factor_one<T, G, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+    } else if (ln.cls == CLS_S) {
       // one case per thread, fronts up to 8 x 9
       const int tpb = sizeof(T) == 8 ? 4 : 8;
       launch_factor_one<T, 32, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, tpb);
@@ -510,8 +519,10 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
   const int max_it = h->opt.max_it_nr;
   int it = 0;
   for (;; ++it) {
+    // mismatch and Jacobian in one pass (the last allowed iteration needs no J)
     ev = tm.begin(FAM_MIS);
-    k_mismatch_nr<T><<<rg, 256, 0, st>>>(d, x);
+    if (it < max_it) k_mismatch_nr<T, true><<<rg, 256, 0, st>>>(d, x, A);
+    else k_mismatch_nr<T, false><<<rg, 256, 0, st>>>(d, x, A);
     CUDA_TRY(cudaGetLastError());
     ++nl;
     tm.end(ev);
@@ -519,11 +530,6 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
     check(h, st, it, max_it, &nl);
     tm.end(ev);
     if (it >= max_it || !any_active(h, st)) break;
-    ev = tm.begin(FAM_JAC);
-    k_jfill<T><<<rg, 256, 0, st>>>(d, A);
-    CUDA_TRY(cudaGetLastError());
-    ++nl;
-    tm.end(ev);
     ev = tm.begin(FAM_FACT);
     launch_factor<T>(J, h->ngroups, A, pan, cb, cbr, x, d.status, d.group_active, 1, st, &nl);
     tm.end(ev);

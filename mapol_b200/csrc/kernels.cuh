@@ -8,10 +8,10 @@
 //
 // Per Newton iteration (newtonpf.h:365-523 does the same steps for one case):
 //   k_mismatch_nr   Ibus = Ybus V, mis = V conj(Ibus) - Sbus, F into the LU
-//                   right-hand side, per-case max |F|       (newtonpf.h:18-95)
+//                   right-hand side, per-case max |F|       (newtonpf.h:18-95),
+//                   and in the same pass the Jacobian entries straight into the
+//                   factor input (A-array)                  (newtonpf.h:97-186)
 //   k_check         per-case convergence / iteration-limit / divergence mask
-//   k_jfill         Jacobian entries straight into the factor input (A-array)
-//                                                           (newtonpf.h:97-186)
 //   k_mf_factor     multifrontal LU of all cases, level by level, forward
 //                   substitution of F carried through the fronts
 //   k_mf_bsolve     backward substitution, level by level (top down)
@@ -183,8 +183,11 @@ __global__ void k_check(DevGrid d, int it, int max_it, double tol) {
 // grid (row blocks, groups); 8 warps per block; a warp = one bus row x 32 cases.
 constexpr int kRowsPerBlock = 64;
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x) {
+// With JAC, the same warp then writes the Jacobian entries of its row (see k_jfill
+// for the formulas), reusing the row's admittances, voltages and Ibus; the
+// Jacobian of a case that converges on this mismatch is simply not used.
+template <typename T, bool JAC>
+__global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x, T* A) {
   const int g = blockIdx.y;
   if (!d.group_active[g]) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -196,7 +199,8 @@ __global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x) {
   for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
     const int i = d.mis_rows[r];
     double2 ib = make_double2(0.0, 0.0);
-    for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
+    const int p0 = d.y_rowptr[i], p1 = d.y_rowptr[i + 1];
+    for (int p = p0; p < p1; ++p) {
       const double2 y = ycase(d, o, p, d.y_val[p]);
       const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
       ib.x += y.x * v.x - y.y * v.y;
@@ -207,7 +211,6 @@ __global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x) {
     // mis = V conj(Ibus) - S
     const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
     const double mi = vi.y * ib.x - vi.x * ib.y - s.y;
-    d.Ibus[at32(g, d.nb, i, lane)] = ib;
     const int2 jv = d.jvar[i];
     x[at32(g, d.n_jac, jv.x, lane)] = (T)mr;
     double m = fabs(mr);
@@ -218,6 +221,29 @@ __global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x) {
     }
     if (mr != mr) m = INFINITY;
     lmax = fmax(lmax, finite_or_inf(m));
+    if (JAC) {
+      const double a = vi.x, b = vi.y;
+      for (int p = p0; p < p1; ++p) {
+        const int4 jp = d.jpos[p];
+        if (jp.x < 0 && jp.y < 0 && jp.z < 0 && jp.w < 0) continue;
+        const int j = d.y_col[p];
+        const double2 y = ycase(d, o, p, d.y_val[p]);
+        const double2 vj = d.V[at32(g, d.nb, j, lane)];
+        const double cc = vj.x, dd = vj.y;
+        const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
+        const double ir = (i == j) ? ib.x : 0.0, ii = (i == j) ? ib.y : 0.0;
+        if (jp.x >= 0) A[at32(g, d.nA_jac, jp.x, lane)] = (T)(-b * (ir - yvr) - a * (-ii + yvi));
+        if (jp.z >= 0) A[at32(g, d.nA_jac, jp.z, lane)] = (T)(-b * (-ii + yvi) + a * (ir - yvr));
+        if (jp.y >= 0 || jp.w >= 0) {
+          const double ab = sqrt(cc * cc + dd * dd);
+          const double wr = yvr / ab, wi = yvi / ab;
+          if (jp.y >= 0) A[at32(g, d.nA_jac, jp.y, lane)] = (T)(a * wr + b * wi + (ir * cc + ii * dd) / ab);
+          if (jp.w >= 0) A[at32(g, d.nA_jac, jp.w, lane)] = (T)(-a * wi + b * wr + (ir * dd - ii * cc) / ab);
+        }
+      }
+    } else {
+      d.Ibus[at32(g, d.nb, i, lane)] = ib;
+    }
   }
   block_lane_max(lmax, &d.facc[c], d.status[c] == ST_RUNNING);
 }
