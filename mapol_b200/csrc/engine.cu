@@ -228,6 +228,19 @@ void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const
 // Warp teams need enough tasks to fill the GPU; a launch with fewer tasks gives
 // each front a 256-thread team instead (8x the threads on the same chain of pivots).
 constexpr long long kMinWarpTasks = 148LL * 24;
+// block teams: aim for at least four resident blocks' worth of tasks per SM
+constexpr long long kMinBlockTasks = 148LL * 4;
+
+template <typename T>
+void launch_factor_ge(int ge, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr,
+                      T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
+  switch (ge) {
+    case 8: launch_factor_one<T, 8, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
+    case 4: launch_factor_one<T, 4, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
+    case 2: launch_factor_one<T, 2, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
+    default: launch_factor_one<T, 1, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
+  }
+}
 
 template <typename T>
 void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x, int* status,
@@ -238,7 +251,9 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
     if (ln.cls == CLS_S && lanes_tasks < kMinWarpTasks) {
       launch_factor_one<T, 32, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
     } else if ((ln.cls == CLS_M1 || ln.cls == CLS_M) && lanes_tasks * (32 / G) < kMinWarpTasks) {
-      launch_factor_one<T, G, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+      int ge = G;
+      while (ge > 1 && lanes_tasks * (32 / ge) < kMinBlockTasks) ge /= 2;
+      launch_factor_ge<T>(ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
     } else if (ln.cls == CLS_S) {
       // one case per thread, fronts up to 8 x 9
       const int tpb = sizeof(T) == 8 ? 4 : 8;
@@ -248,15 +263,13 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
     } else if (ln.cls == CLS_M) {
       launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 4);
     } else {
+      // large fronts: 256-thread team per chunk of Ge lanes; Ge shrinks (more,
+      // smaller tasks) when the level has too few tasks to fill the GPU or when a
+      // 32-byte chunk of the front would not fit in shared memory
       const size_t per_lane = (size_t)ln.fcap * front_stride(ln.fcap) * sizeof(T);
-      if (per_lane * G <= kSmemMax)
-        launch_factor_one<T, G, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
-      else if (per_lane * (G / 2) <= kSmemMax)
-        launch_factor_one<T, G / 2, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
-      else if (per_lane * (G / 4) <= kSmemMax)
-        launch_factor_one<T, G / 4, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
-      else
-        launch_factor_one<T, 1, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+      int ge = G;
+      while (ge > 1 && (per_lane * ge > kSmemMax || lanes_tasks * (32 / ge) < kMinBlockTasks)) ge /= 2;
+      launch_factor_ge<T>(ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
     }
     ++*nlaunch;
   }
@@ -269,7 +282,10 @@ void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const i
   static bool attr_set = false;
   if (!attr_set) {
     CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     attr_set = true;
   }
   for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
@@ -282,11 +298,21 @@ void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const i
       k_mf_bsolve<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
                                                           ngroups, ln.fcap, pan, x, group_active);
     } else {
-      const long long ntasks = (long long)ln.count * ngroups * (32 / G);
+      // chunked: fewer lanes per warp (more warps, more slots per lane) on levels
+      // with few supernodes
+      int ge = G;
+      while (ge > 1 && (long long)ln.count * ngroups * (32 / ge) < 148LL * 16) ge /= 2;
+      const long long ntasks = (long long)ln.count * ngroups * (32 / ge);
       const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-      const size_t smem = (size_t)4 * ln.fcap * G * sizeof(T);
-      k_mf_bsolve_chunk<T, G><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset,
-                                                                   ln.count, ngroups, ln.fcap, pan, x, group_active);
+      const size_t smem = (size_t)4 * ln.fcap * ge * sizeof(T);
+      const DevLU dl = sys.dev();
+      const int* ts = sys.lev_sn.as<int>() + ln.offset;
+      switch (ge) {
+        case 8: k_mf_bsolve_chunk<T, 8><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+        case 4: k_mf_bsolve_chunk<T, 4><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+        case 2: k_mf_bsolve_chunk<T, 2><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+        default: k_mf_bsolve_chunk<T, 1><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+      }
     }
     CUDA_TRY(cudaGetLastError());
     ++*nlaunch;
