@@ -206,16 +206,36 @@ struct Prec<double> { static constexpr int idx = 0; static constexpr int G = 4; 
 template <>
 struct Prec<float> { static constexpr int idx = 1; static constexpr int G = 8; };
 
+// Opt every kernel that may take more than 48 KB of dynamic shared memory into the
+// full 227 KB, once per device and value type, before any launch or graph capture.
+template <typename T>
+void ensure_attrs(int device) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= 64 || done[device]) return;
+  const int smax = (int)kSmemMax;
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 32, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 8, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 1, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_fsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  done[device] = true;
+}
+
 template <typename T, int G, int TEAM>
 void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x,
                        int* status, const int* group_active, int with_rhs, cudaStream_t st, int teams_per_block) {
   const size_t team_elems = (size_t)ln.fcap * front_stride(ln.fcap) * G;
   const size_t smem = team_elems * sizeof(T) * teams_per_block;
-  static bool attr_set = false;
-  if (!attr_set) {
-    CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, G, TEAM>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attr_set = true;
-  }
   const long long ntasks = (long long)ln.count * ngroups * (32 / G);
   long long blocks = (ntasks + teams_per_block - 1) / teams_per_block;
   blocks = std::min<long long>(blocks, 148LL * 32);
@@ -279,15 +299,6 @@ template <typename T>
 void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active, cudaStream_t st,
                    int* nlaunch) {
   constexpr int G = Prec<T>::G;
-  static bool attr_set = false;
-  if (!attr_set) {
-    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attr_set = true;
-  }
   for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
     const Launch& ln = sys.level_sched[k];
     if (ln.fcap <= kFmaxM1) {
@@ -322,11 +333,6 @@ void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const i
 template <typename T>
 void launch_fsolve(const LUSystem& sys, int ngroups, const T* pan, T* cbr, T* x, const int* group_active,
                    cudaStream_t st, int* nlaunch) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    CUDA_TRY(cudaFuncSetAttribute(k_mf_fsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attr_set = true;
-  }
   for (const Launch& ln : sys.level_sched) {
     const long long ntasks = (long long)ln.count * ngroups;
     long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
@@ -397,7 +403,7 @@ struct mpf_handle {
   bool fd_ready[2] = {false, false};
   // cases
   int ncases = 0, ngroups = 0, maxk = 0;
-  DevBuf out_br, sbus_case, V, Ibus, status, iters, maxmis, facc, group_active, any_active;
+  DevBuf out_br, sbus_case, V, Ibus, status, iters, maxmis, facc, group_active, any_active, it_ctr;
   DevBuf vout, small_out;
   DevBuf eval_acc;  // mpf_mismatch accumulator, allocated on first use
   bool have_cases = false, have_results = false;
@@ -406,6 +412,22 @@ struct mpf_handle {
   int* h_any = nullptr;  // pinned
   EventTimer timer;
   mpf_timing timing;
+  // captured Newton iteration per precision [FP64, FP32]
+  struct IterGraph {
+    cudaGraph_t graph[4] = {};
+    cudaGraphExec_t exec[4] = {};
+    const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
+    int ngroups = 0, launches[4] = {0, 0, 0, 0};
+    void release() {
+      for (int k = 0; k < 4; ++k) {
+        if (exec[k]) cudaGraphExecDestroy(exec[k]);
+        if (graph[k]) cudaGraphDestroy(graph[k]);
+        exec[k] = nullptr;
+        graph[k] = nullptr;
+      }
+      ngroups = 0;
+    }
+  } nr_graph[2];
   cudaEvent_t t0 = nullptr, t1 = nullptr;
 
   DevGrid dev() const {
@@ -436,6 +458,7 @@ struct mpf_handle {
     d.facc = facc.as<unsigned long long>();
     d.group_active = group_active.as<int>();
     d.any_active = any_active.as<int>();
+    d.it_ptr = it_ctr.as<int>();
     return d;
   }
 
@@ -443,7 +466,7 @@ struct mpf_handle {
     size_t b = 0;
     const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
                            &out_br, &sbus_case, &V, &Ibus, &status, &iters, &maxmis, &facc, &group_active,
-                           &any_active, &vout, &small_out, &fdvar, &eval_acc};
+                           &any_active, &vout, &small_out, &fdvar, &eval_acc, &it_ctr};
     for (auto p : all) b += p->bytes;
     const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
     for (auto s : systems) {
@@ -523,6 +546,37 @@ void check(mpf_handle* h, cudaStream_t st, int it, int max_it, int* nl) {
   ++*nl;
 }
 
+// One Newton iteration after a check that left cases running, in four parts:
+//   0 factorisation with the forward substitution fused
+//   1 backward substitution
+//   2 voltage update
+//   3 the next mismatch (with the Jacobian of the new point) and its check
+template <typename T>
+int enqueue_nr_part(mpf_handle* h, int part, cudaStream_t st, T* A, T* pan, T* cb, T* cbr, T* x) {
+  LUSystem& J = h->jac;
+  const DevGrid d = h->dev();
+  const dim3 rg = row_grid(h);
+  int nl = 0;
+  if (part == 0) {
+    launch_factor<T>(J, h->ngroups, A, pan, cb, cbr, x, d.status, d.group_active, 1, st, &nl);
+  } else if (part == 1) {
+    launch_bsolve<T>(J, h->ngroups, pan, x, d.group_active, st, &nl);
+  } else if (part == 2) {
+    k_update_nr<T><<<rg, 256, 0, st>>>(d, x);
+    CUDA_TRY(cudaGetLastError());
+    ++nl;
+  } else {
+    k_mismatch_nr<T, true><<<rg, 256, 0, st>>>(d, x, A);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemsetAsync(h->any_active.p, 0, sizeof(int), st));
+    const int nl_lanes = h->ngroups * 32;
+    k_check<<<(nl_lanes + 255) / 256, 256, 0, st>>>(d, -1, h->opt.max_it_nr, h->opt.tol);
+    CUDA_TRY(cudaGetLastError());
+    nl += 2;
+  }
+  return nl;
+}
+
 template <typename T>
 void solve_nr(mpf_handle* h, cudaStream_t st) {
   constexpr int P = Prec<T>::idx;
@@ -543,30 +597,49 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
   ++nl;
   tm.end(ev);
   const int max_it = h->opt.max_it_nr;
+  ev = tm.begin(FAM_MIS);
+  if (max_it > 0) k_mismatch_nr<T, true><<<rg, 256, 0, st>>>(d, x, A);
+  else k_mismatch_nr<T, false><<<rg, 256, 0, st>>>(d, x, A);
+  CUDA_TRY(cudaGetLastError());
+  ++nl;
+  tm.end(ev);
+  ev = tm.begin(FAM_OTHER);
+  check(h, st, 0, max_it, &nl);
+  tm.end(ev);
+  static const int kFam[4] = {FAM_FACT, FAM_SOLVE, FAM_UPD, FAM_MIS};
   int it = 0;
-  for (;; ++it) {
-    // mismatch and Jacobian in one pass (the last allowed iteration needs no J)
-    ev = tm.begin(FAM_MIS);
-    if (it < max_it) k_mismatch_nr<T, true><<<rg, 256, 0, st>>>(d, x, A);
-    else k_mismatch_nr<T, false><<<rg, 256, 0, st>>>(d, x, A);
-    CUDA_TRY(cudaGetLastError());
-    ++nl;
-    tm.end(ev);
-    ev = tm.begin(FAM_OTHER);
-    check(h, st, it, max_it, &nl);
-    tm.end(ev);
-    if (it >= max_it || !any_active(h, st)) break;
-    ev = tm.begin(FAM_FACT);
-    launch_factor<T>(J, h->ngroups, A, pan, cb, cbr, x, d.status, d.group_active, 1, st, &nl);
-    tm.end(ev);
-    ev = tm.begin(FAM_SOLVE);
-    launch_bsolve<T>(J, h->ngroups, pan, x, d.group_active, st, &nl);
-    tm.end(ev);
-    ev = tm.begin(FAM_UPD);
-    k_update_nr<T><<<rg, 256, 0, st>>>(d, x);
-    CUDA_TRY(cudaGetLastError());
-    ++nl;
-    tm.end(ev);
+  auto& gph = h->nr_graph[P];
+  if (h->opt.use_graph) {
+    const void* key[4] = {A, pan, cb, x};
+    if (gph.exec[0] && (gph.ngroups != h->ngroups || std::memcmp(gph.key, key, sizeof(key)) != 0)) gph.release();
+    if (!gph.exec[0]) {
+      // capture each part on a private stream (the caller's may be the legacy one)
+      cudaStream_t cs;
+      CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      for (int part = 0; part < 4; ++part) {
+        CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        gph.launches[part] = enqueue_nr_part<T>(h, part, cs, A, pan, cb, cbr, x);
+        CUDA_TRY(cudaStreamEndCapture(cs, &gph.graph[part]));
+        CUDA_TRY(cudaGraphInstantiate(&gph.exec[part], gph.graph[part], 0));
+      }
+      CUDA_TRY(cudaStreamDestroy(cs));
+      std::memcpy(gph.key, key, sizeof(key));
+      gph.ngroups = h->ngroups;
+    }
+  }
+  while (it < max_it && any_active(h, st)) {
+    int e[4];
+    for (int part = 0; part < 4; ++part) {
+      e[part] = tm.begin(kFam[part]);
+      if (h->opt.use_graph) {
+        CUDA_TRY(cudaGraphLaunch(gph.exec[part], st));
+        nl += gph.launches[part];
+      } else {
+        nl += enqueue_nr_part<T>(h, part, st, A, pan, cb, cbr, x);
+      }
+      tm.end(e[part]);
+    }
+    ++it;
   }
   h->timing.launches = nl;
   h->timing.iterations_max = it;
@@ -788,6 +861,7 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
     }
     h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac);
     h->any_active.alloc(sizeof(int));
+    h->it_ctr.alloc(sizeof(int));
     return MPF_OK;
   });
   *out = h.release();
@@ -801,6 +875,7 @@ int32_t mpf_destroy(mpf_handle* h) {
     cudaStreamSynchronize(h->own_stream);
     cudaStreamDestroy(h->own_stream);
   }
+  for (auto& gph : h->nr_graph) gph.release();
   if (h->h_any) cudaFreeHost(h->h_any);
   if (h->t0) cudaEventDestroy(h->t0);
   if (h->t1) cudaEventDestroy(h->t1);
@@ -923,6 +998,8 @@ int32_t mpf_solve(mpf_handle* h, int32_t alg, int32_t precision, void* stream) {
     std::memset(&h->timing, 0, sizeof(h->timing));
     h->timer.reset(st);
     CUDA_TRY(cudaEventRecord(h->t0, st));
+    ensure_attrs<double>(h->device);
+    ensure_attrs<float>(h->device);
     if (alg == MPF_NR) {
       if (precision == MPF_FP64) solve_nr<double>(h, st);
       else solve_nr<float>(h, st);

@@ -59,6 +59,7 @@ struct DevGrid {
   unsigned long long* facc; // running max |F| (bits of a non-negative double)
   int* group_active;        // [ngroups]
   int* any_active;          // [1]
+  int* it_ptr;              // [1] Newton iterations done (graph replays read it)
 };
 
 struct DevLU {
@@ -151,12 +152,15 @@ __global__ void k_init(DevGrid d, int ncases) {
   }
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < d.ngroups; g += gridDim.x * blockDim.x)
     d.group_active[g] = 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d.it_ptr = 0;
 }
 
 // One thread per case (a warp = a group): decide convergence of the mismatch just
-// evaluated.  it = iterations done so far; the reference loop stops when
-// max |F| < tol or it == max_it (newtonpf.h:394-398, 518).
-__global__ void k_check(DevGrid d, int it, int max_it, double tol) {
+// evaluated.  it = iterations done so far (it_arg, or the device counter when
+// it_arg < 0); the reference loop stops when max |F| < tol or it == max_it
+// (newtonpf.h:394-398, 518).
+__global__ void k_check(DevGrid d, int it_arg, int max_it, double tol) {
+  const int it = it_arg >= 0 ? it_arg : *d.it_ptr;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int nl = d.ngroups * 32;
   bool active = false;
@@ -291,6 +295,7 @@ __global__ void __launch_bounds__(256) k_jfill(DevGrid d, T* A) {
 // ---------------------------------------------------------------- Newton update
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_nr(DevGrid d, const T* x) {
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(d.it_ptr, 1);  // one more iteration
   const int g = blockIdx.y;
   if (!d.group_active[g]) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -198,3 +198,41 @@ def test_mismatch_entry_point_matches_solve_and_oracle(gpu):
     for k in (0, 7, 31):
         _, _, err = oracle.nr_system(buses, branches, flat[k], cases[k])
         assert abs(got[k] - err) <= 1e-12 * max(1.0, err)
+
+
+def test_graph_and_direct_launches_agree(gpu):
+    """The graph-captured iteration (default) and direct launches give identical
+    results, and replays after set_cases with a different batch size rebuild it."""
+    buses, branches, cases = m.workload("cfg1_300bus")
+    out = []
+    for use_graph in (1, 0):
+        pf = m.PowerFlow(buses, branches)
+        pf_opt = pf  # noqa: F841
+        pf.close()
+        from mapol_b200 import _types as T
+        from mapol_b200._lib import lib, ptr
+        import ctypes
+
+        opt = T.Options()
+        lib().mpf_default_options(ctypes.byref(opt))
+        opt.use_graph = use_graph
+        h = ctypes.c_void_p()
+        assert lib().mpf_create(ptr(buses), len(buses), ptr(branches), len(branches), ctypes.byref(opt),
+                                ctypes.byref(h)) == 0
+        res = []
+        for n in (200, 45, 200):
+            from mapol_b200.grid import cases_to_offsets
+
+            offs, flat = cases_to_offsets(cases[:n])
+            assert lib().mpf_set_cases(h, n, ptr(offs), ptr(flat), None) == 0
+            for prec in (m.FP64, m.MIXED):
+                assert lib().mpf_solve(h, m.NR, prec, None) == 0
+                v = np.zeros((n, len(buses), 2))
+                it = np.zeros(n, np.int32)
+                assert lib().mpf_get_results(h, ptr(v), ptr(it), None, None) == 0
+                res.append((v.copy(), it.copy()))
+        lib().mpf_destroy(h)
+        out.append(res)
+    for (va, ia), (vb, ib) in zip(out[0], out[1]):
+        assert np.array_equal(ia, ib)
+        assert np.array_equal(va, vb)
