@@ -395,7 +395,7 @@ struct mpf_handle {
   cudaStream_t own_stream = nullptr;
   GridSymbolic g;
   // shared device arrays
-  DevBuf y_rowptr, y_col, y_val, br_ypos, br_y, sbus0, v0, mis_rows, jvar, jpos;
+  DevBuf y_rowptr, y_col, y_val, y_diag, br_ypos, br_y, sbus0, v0, mis_rows, jvar, jpos;
   LUSystem jac;
   LUSystem bp[2], bpp[2];
   FDData fdp[2], fdpp[2];
@@ -441,6 +441,7 @@ struct mpf_handle {
     d.y_rowptr = y_rowptr.as<int>();
     d.y_col = y_col.as<int>();
     d.y_val = y_val.as<double2>();
+    d.y_diag = y_diag.as<int>();
     d.br_ypos = br_ypos.as<int4>();
     d.br_y = br_y.as<double2>();
     d.sbus0 = sbus0.as<double2>();
@@ -464,7 +465,7 @@ struct mpf_handle {
 
   size_t device_bytes() const {
     size_t b = 0;
-    const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
+    const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &y_diag, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
                            &out_br, &sbus_case, &V, &Ibus, &status, &iters, &maxmis, &facc, &group_active,
                            &any_active, &vout, &small_out, &fdvar, &eval_acc, &it_ctr};
     for (auto p : all) b += p->bytes;
@@ -831,6 +832,7 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
     CUDA_TRY(cudaEventCreate(&h->t1));
     upload(h->y_rowptr, g.y_rowptr);
     upload(h->y_col, g.y_col);
+    upload(h->y_diag, g.y_diag);
     {
       std::vector<double2> yv(g.y_val.size() / 2);
       for (size_t k = 0; k < yv.size(); ++k) yv[k] = make_double2(g.y_val[2 * k], g.y_val[2 * k + 1]);

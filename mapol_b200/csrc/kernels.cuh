@@ -42,6 +42,7 @@ struct DevGrid {
   const int* y_rowptr;
   const int* y_col;
   const double2* y_val;
+  const int* y_diag;        // [nb] position of (i, i)
   const int4* br_ypos;      // per branch: Ybus positions (ff, ft, tf, tt)
   const double2* br_y;      // per branch: 4 admittances
   const double2* sbus0;     // [nb]
@@ -86,9 +87,12 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+// A lane's outaged branches: their indices and end buses.  An outage only changes
+// the Ybus rows of its two end buses, so a row whose bus is neither end reads the
+// base Ybus unchanged.
 struct LaneOut {
   int e[kMaxOut];
-  int4 pos[kMaxOut];
+  int2 ft[kMaxOut];
 };
 
 __device__ __forceinline__ void load_outages(const DevGrid& d, int c, LaneOut& o) {
@@ -96,8 +100,24 @@ __device__ __forceinline__ void load_outages(const DevGrid& d, int c, LaneOut& o
 #pragma unroll
   for (int k = 0; k < kMaxOut; ++k) {
     o.e[k] = d.out_br[k * stride + c];
-    o.pos[k] = o.e[k] >= 0 ? d.br_ypos[o.e[k]] : make_int4(-1, -1, -1, -1);
+    if (o.e[k] >= 0) {
+      const int4 q = d.br_ypos[o.e[k]];
+      // positions ff (diagonal of from) and tt (diagonal of to) identify the end
+      // buses' rows; the row of a position is found by the caller's row index
+      o.ft[k] = make_int2(q.x, q.w);
+    } else {
+      o.ft[k] = make_int2(-1, -1);
+    }
   }
+}
+
+// True when row i (whose diagonal Ybus position is pdiag) belongs to an end bus of
+// one of the lane's outaged branches.
+__device__ __forceinline__ bool row_touched(const LaneOut& o, int pdiag) {
+  bool t = false;
+#pragma unroll
+  for (int k = 0; k < kMaxOut; ++k) t |= (o.ft[k].x == pdiag) | (o.ft[k].y == pdiag);
+  return t;
 }
 
 // Ybus entry p of this case: base value minus the outaged branches' parts
@@ -106,7 +126,7 @@ __device__ __forceinline__ double2 ycase(const DevGrid& d, const LaneOut& o, int
 #pragma unroll
   for (int k = 0; k < kMaxOut; ++k) {
     if (o.e[k] < 0) continue;
-    const int4 q = o.pos[k];
+    const int4 q = d.br_ypos[o.e[k]];
     const double2* by = d.br_y + 4 * o.e[k];
     if (p == q.x) { const double2 t = by[0]; y.x -= t.x; y.y -= t.y; }
     if (p == q.y) { const double2 t = by[1]; y.x -= t.x; y.y -= t.y; }
@@ -187,11 +207,15 @@ __global__ void k_check(DevGrid d, int it_arg, int max_it, double tol) {
 // grid (row blocks, groups); 8 warps per block; a warp = one bus row x 32 cases.
 constexpr int kRowsPerBlock = 64;
 
-// With JAC, the same warp then writes the Jacobian entries of its row (see k_jfill
-// for the formulas), reusing the row's admittances, voltages and Ibus; the
-// Jacobian of a case that converges on this mismatch is simply not used.
+// With JAC, the same warp then writes the Jacobian entries of its row, reusing the
+// row's admittances, voltages and Ibus; the Jacobian of a case that converges on
+// this mismatch is simply not used.
+// J block entries of Ybus entry (i, j) in rectangular form (newtonpf.h:97-186):
+//   V_i = a + jb, V_j = c + jd, yv = Y_ij V_j, w = yv / |V_j|, I = Ibus_i if i == j else 0
+//   dP/dVa = -b (I_r - yv_r) - a (-I_i + yv_i)     dP/dVm = a w_r + b w_i + (I_r c + I_i d)/|V_j|
+//   dQ/dVa = -b (-I_i + yv_i) + a (I_r - yv_r)     dQ/dVm = -a w_i + b w_r + (I_r d - I_i c)/|V_j|
 template <typename T, bool JAC>
-__global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x, T* A) {
+__global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
   const int g = blockIdx.y;
   if (!d.group_active[g]) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -204,8 +228,9 @@ __global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x, T* A) {
     const int i = d.mis_rows[r];
     double2 ib = make_double2(0.0, 0.0);
     const int p0 = d.y_rowptr[i], p1 = d.y_rowptr[i + 1];
+    const bool touched = row_touched(o, d.y_diag[i]);
     for (int p = p0; p < p1; ++p) {
-      const double2 y = ycase(d, o, p, d.y_val[p]);
+      const double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
       const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
       ib.x += y.x * v.x - y.y * v.y;
       ib.y += y.x * v.y + y.y * v.x;
@@ -231,7 +256,7 @@ __global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x, T* A) {
         const int4 jp = d.jpos[p];
         if (jp.x < 0 && jp.y < 0 && jp.z < 0 && jp.w < 0) continue;
         const int j = d.y_col[p];
-        const double2 y = ycase(d, o, p, d.y_val[p]);
+        const double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
         const double2 vj = d.V[at32(g, d.nb, j, lane)];
         const double cc = vj.x, dd = vj.y;
         const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
@@ -250,46 +275,6 @@ __global__ void __launch_bounds__(256) k_mismatch_nr(DevGrid d, T* x, T* A) {
     }
   }
   block_lane_max(lmax, &d.facc[c], d.status[c] == ST_RUNNING);
-}
-
-// ---------------------------------------------------------------- Jacobian fill
-// J block entries of Ybus entry (i, j) in rectangular form (newtonpf.h:97-186):
-//   V_i = a + jb, V_j = c + jd, yv = Y_ij V_j, w = yv / |V_j|, I = Ibus_i if i == j else 0
-//   dP/dVa = -b (I_r - yv_r) - a (-I_i + yv_i)     dP/dVm = a w_r + b w_i + (I_r c + I_i d)/|V_j|
-//   dQ/dVa = -b (-I_i + yv_i) + a (I_r - yv_r)     dQ/dVm = -a w_i + b w_r + (I_r d - I_i c)/|V_j|
-template <typename T>
-__global__ void __launch_bounds__(256) k_jfill(DevGrid d, T* A) {
-  const int g = blockIdx.y;
-  if (!d.group_active[g]) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int c = g * 32 + lane;
-  LaneOut o;
-  load_outages(d, c, o);
-  const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
-  for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
-    const int i = d.mis_rows[r];
-    const double2 vi = d.V[at32(g, d.nb, i, lane)];
-    const double2 ibus = d.Ibus[at32(g, d.nb, i, lane)];
-    const double a = vi.x, b = vi.y;
-    for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
-      const int4 jp = d.jpos[p];
-      if (jp.x < 0 && jp.y < 0 && jp.z < 0 && jp.w < 0) continue;
-      const int j = d.y_col[p];
-      const double2 y = ycase(d, o, p, d.y_val[p]);
-      const double2 vj = d.V[at32(g, d.nb, j, lane)];
-      const double cc = vj.x, dd = vj.y;
-      const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
-      const double ir = (i == j) ? ibus.x : 0.0, ii = (i == j) ? ibus.y : 0.0;
-      if (jp.x >= 0) A[at32(g, d.nA_jac, jp.x, lane)] = (T)(-b * (ir - yvr) - a * (-ii + yvi));
-      if (jp.z >= 0) A[at32(g, d.nA_jac, jp.z, lane)] = (T)(-b * (-ii + yvi) + a * (ir - yvr));
-      if (jp.y >= 0 || jp.w >= 0) {
-        const double ab = sqrt(cc * cc + dd * dd);
-        const double wr = yvr / ab, wi = yvi / ab;
-        if (jp.y >= 0) A[at32(g, d.nA_jac, jp.y, lane)] = (T)(a * wr + b * wi + (ir * cc + ii * dd) / ab);
-        if (jp.w >= 0) A[at32(g, d.nA_jac, jp.w, lane)] = (T)(-a * wi + b * wr + (ir * dd - ii * cc) / ab);
-      }
-    }
-  }
 }
 
 // ---------------------------------------------------------------- Newton update
@@ -337,8 +322,9 @@ __global__ void __launch_bounds__(256) k_mismatch_fd(DevGrid d, DevFD f, T* xp, 
   for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
     const int i = d.mis_rows[r];
     double2 ib = make_double2(0.0, 0.0);
+    const bool touched = row_touched(o, d.y_diag[i]);
     for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
-      const double2 y = ycase(d, o, p, d.y_val[p]);
+      const double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
       const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
       ib.x += y.x * v.x - y.y * v.y;
       ib.y += y.x * v.y + y.y * v.x;
@@ -659,8 +645,9 @@ __global__ void __launch_bounds__(256) k_mismatch_eval(DevGrid d, const double2*
     const double2* vc = v + (size_t)c * d.nb;
     const int i = d.mis_rows[r];
     double2 ib = make_double2(0.0, 0.0);
+    const bool touched = row_touched(o, d.y_diag[i]);
     for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
-      const double2 y = ycase(d, o, p, d.y_val[p]);
+      const double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
       const double2 vj = vc[d.y_col[p]];
       ib.x += y.x * vj.x - y.y * vj.y;
       ib.y += y.x * vj.y + y.y * vj.x;
