@@ -215,6 +215,34 @@ int32_t mpf_mismatch(mpf_handle* h, const double* v, double* max_mis, void* stre
  * streams, or different handles on the same device) race and must be serialised. */
 int32_t mpf_mismatch_noalloc(mpf_handle* h, const double* v, double* max_mis, void* stream);
 
+/* Branch ratings (host array [n_branch], p.u. of apparent power; NULL clears them),
+ * used by the overload term of mpf_branch_flows and by mpf_adjoint. */
+int32_t mpf_set_ratings(mpf_handle* h, const double* rating);
+
+/* Branch flows at the solved voltages of the last mpf_solve, every case:
+ *   ploss    device [n_cases]: total active loss sum_k Re(Sf_k + St_k), the quantity
+ *            mkl_computeLoss / hybrid_computeLoss + reduceLoss return per case
+ *            (src/powerflow/runpf.h:228-257, 543-604)
+ *   overload device [n_cases] or NULL: sum_k relu(|Sf_k| - 0.9 rating_k)^2 (needs ratings)
+ *   sf, st   device [n_cases][n_branch][2] or NULL: from-/to-end complex power
+ * Sf = Vf conj(Yff Vf + Yft Vt), St = Vt conj(Ytf Vf + Ytt Vt); an outaged branch
+ * carries nothing.  The caller decides which cases count (the reference uses
+ * DBL_MAX for cases that did not converge, runpf.h:782-789). */
+int32_t mpf_branch_flows(mpf_handle* h, double* ploss, double* overload, double* sf, double* st, void* stream);
+
+/* Adjoint gradients of each converged case's overload loss
+ *   L = sum_k relu(|Sf_k| - 0.9 rating_k)^2        (needs mpf_set_ratings)
+ * at the solved voltages of the last mpf_solve.  J is refactorised at the solution in
+ * `precision` (MPF_FP64 or MPF_MIXED = FP32 factors) and J^T lambda = dL/dx is solved
+ * with transposed substitutions on those factors.  Outputs (device, each nullable):
+ *   grad_p, grad_q [n_cases][n_bus]     dL/dP, dL/dQ of the net injections (0 where the
+ *                                       injection is not a Newton equation: slack, Q of PV)
+ *   grad_g, grad_b [n_cases][n_branch]  dL/dg, dL/db of the series admittance g + jb =
+ *                                       1/(r + jx) (0 for outaged branches)
+ * Cases that did not converge get zero gradients.  No counterpart in the reference. */
+int32_t mpf_adjoint(mpf_handle* h, int32_t precision, double* grad_p, double* grad_q, double* grad_g,
+                    double* grad_b, void* stream);
+
 /* Device time per kernel family of the last solve (synchronises the solve stream). */
 int32_t mpf_get_timing(mpf_handle* h, mpf_timing* t);
 

@@ -34,6 +34,9 @@ _SIGNATURES = {
     "mpf_get_timing": (c_i32, [c_p, ctypes.POINTER(T.Timing)]),
     "mpf_mismatch": (c_i32, [c_p, c_p, c_p, c_p]),
     "mpf_mismatch_noalloc": (c_i32, [c_p, c_p, c_p, c_p]),
+    "mpf_set_ratings": (c_i32, [c_p, c_p]),
+    "mpf_branch_flows": (c_i32, [c_p, c_p, c_p, c_p, c_p, c_p]),
+    "mpf_adjoint": (c_i32, [c_p, c_i32, c_p, c_p, c_p, c_p, c_p]),
     "mpf_synth_default": (None, [ctypes.POINTER(T.SynthParams)]),
     "mpf_synth_grid": (c_i32, [ctypes.POINTER(T.SynthParams), c_p, c_p]),
     "mpf_find_bridges": (c_i32, [c_p, c_i32, c_i32, c_p]),

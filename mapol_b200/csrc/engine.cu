@@ -395,7 +395,7 @@ struct mpf_handle {
   cudaStream_t own_stream = nullptr;
   GridSymbolic g;
   // shared device arrays
-  DevBuf y_rowptr, y_col, y_val, y_diag, br_ypos, br_y, sbus0, v0, mis_rows, jvar, jpos;
+  DevBuf y_rowptr, y_col, y_val, y_diag, br_ft, rating, br_ypos, br_y, sbus0, v0, mis_rows, jvar, jpos;
   LUSystem jac;
   LUSystem bp[2], bpp[2];
   FDData fdp[2], fdpp[2];
@@ -406,6 +406,8 @@ struct mpf_handle {
   DevBuf out_br, sbus_case, V, Ibus, status, iters, maxmis, facc, group_active, any_active, it_ctr;
   DevBuf vout, small_out;
   DevBuf eval_acc;  // mpf_mismatch accumulator, allocated on first use
+  DevBuf br_dy;     // per branch dY/dg for (ff, ft, tf, tt), adjoint
+  DevBuf adj_status;  // statuses the adjoint's refactorisation may write (kept apart)
   bool have_cases = false, have_results = false;
   int last_alg = -1, last_prec = -1;
   cudaStream_t last_stream = nullptr;  // stream of the last solve / result copy
@@ -443,6 +445,7 @@ struct mpf_handle {
     d.y_val = y_val.as<double2>();
     d.y_diag = y_diag.as<int>();
     d.br_ypos = br_ypos.as<int4>();
+    d.br_ft = br_ft.as<int2>();
     d.br_y = br_y.as<double2>();
     d.sbus0 = sbus0.as<double2>();
     d.sbus_case = sbus_case.p ? sbus_case.as<double2>() : nullptr;
@@ -465,9 +468,10 @@ struct mpf_handle {
 
   size_t device_bytes() const {
     size_t b = 0;
-    const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &y_diag, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
+    const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &y_diag, &br_ft, &rating, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
                            &out_br, &sbus_case, &V, &Ibus, &status, &iters, &maxmis, &facc, &group_active,
-                           &any_active, &vout, &small_out, &fdvar, &eval_acc, &it_ctr};
+                           &any_active, &vout, &small_out, &fdvar, &eval_acc, &it_ctr, &br_dy,
+                           &adj_status};
     for (auto p : all) b += p->bytes;
     const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
     for (auto s : systems) {
@@ -764,6 +768,72 @@ cudaError_t noalloc_scratch(int device, unsigned long long** out) {
 }
 }  // namespace
 
+// ------------------------------------------------------------------ adjoint
+template <typename T>
+void launch_fsolve_t(const LUSystem& sys, int ngroups, const T* pan, T* cbr, T* x, const int* group_active,
+                     cudaStream_t st) {
+  for (const Launch& ln : sys.level_sched) {
+    const long long ntasks = (long long)ln.count * ngroups;
+    const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
+    const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
+    k_mf_fsolve_t<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
+                                                          ngroups, ln.fcap, pan, cbr, x, group_active);
+    CUDA_TRY(cudaGetLastError());
+  }
+}
+
+template <typename T>
+void launch_bsolve_t(const LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active, cudaStream_t st) {
+  for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
+    const Launch& ln = sys.level_sched[k];
+    const long long ntasks = (long long)ln.count * ngroups;
+    const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
+    const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
+    k_mf_bsolve_t<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
+                                                          ngroups, ln.fcap, pan, x, group_active);
+    CUDA_TRY(cudaGetLastError());
+  }
+}
+
+// J of the solved point refactorised in T, then J^T lambda = dL/dx by U^T (bottom-up)
+// and L^T (top-down) substitutions, then the bus and branch gradients.
+template <typename T>
+void adjoint_impl(mpf_handle* h, cudaStream_t st, double* gp, double* gq, double* gg, double* gb) {
+  constexpr int P = Prec<T>::idx;
+  LUSystem& J = h->jac;
+  J.ensure_values(P, h->ngroups);
+  T* A = J.A[P].as<T>();
+  T* pan = J.pan[P].as<T>();
+  T* x = J.x[P].as<T>();
+  const int lanes = h->ngroups * 32;
+  if (!h->adj_status.p || h->adj_status.bytes < lanes * sizeof(int)) h->adj_status.alloc(lanes * sizeof(int));
+  DevGrid d = h->dev();
+  k_fill_int<<<(h->ngroups + 255) / 256, 256, 0, st>>>(d.group_active, h->ngroups, 1);
+  CUDA_TRY(cudaGetLastError());
+  const dim3 rg = row_grid(h);
+  k_mismatch_nr<T, true><<<rg, 256, 0, st>>>(d, x, A);
+  CUDA_TRY(cudaGetLastError());
+  int nl = 0;
+  launch_factor<T>(J, h->ngroups, A, pan, J.cb[P].as<T>(), J.cbr[P].as<T>(), x, h->adj_status.as<int>(),
+                   d.group_active, 0, st, &nl);
+  CUDA_TRY(cudaMemsetAsync(x, 0, (size_t)lanes * J.sym.n * sizeof(T), st));
+  const dim3 bg((unsigned)((h->g.nbr + 63) / 64), (unsigned)h->ngroups);
+  k_adj_dldx<T><<<bg, 256, 0, st>>>(d, h->g.nbr, h->rating.as<double>(), x);
+  CUDA_TRY(cudaGetLastError());
+  launch_fsolve_t<T>(J, h->ngroups, pan, J.cbr[P].as<T>(), x, d.group_active, st);
+  launch_bsolve_t<T>(J, h->ngroups, pan, x, d.group_active, st);
+  if (gp || gq) {
+    const size_t total = (size_t)h->ncases * h->g.nb;
+    k_adj_grad_bus<T><<<(unsigned)std::min<size_t>(148 * 16, total / 256 + 1), 256, 0, st>>>(d, h->ncases, x, gp, gq);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (gg || gb) {
+    k_adj_grad_branch<T><<<bg, 256, 0, st>>>(d, h->g.nbr, h->ncases, h->rating.as<double>(),
+                                             h->br_dy.as<double2>(), x, gg, gb);
+    CUDA_TRY(cudaGetLastError());
+  }
+}
+
 // ====================================================================== C-ABI
 extern "C" {
 
@@ -844,6 +914,23 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
         for (int q = 0; q < 4; ++q) by[4 * e + q] = make_double2(g.br_y[8 * e + 2 * q], g.br_y[8 * e + 2 * q + 1]);
       }
       upload(h->br_ypos, bp);
+      std::vector<int2> ft(g.nbr);
+      for (int e = 0; e < g.nbr; ++e) ft[e] = make_int2(g.br_from[e], g.br_to[e]);
+      upload(h->br_ft, ft);
+      // dY/dg of each branch's four entries (series admittance g + jb): 1/|t|^2,
+      // -1/conj(t), -1/t, 1 with t = tap e^{j shift} (tap 0 -> 1); 0 when out of service
+      std::vector<double2> dy(4 * (size_t)g.nbr, make_double2(0.0, 0.0));
+      for (int e = 0; e < g.nbr; ++e) {
+        if (!branches[e].status) continue;
+        const double a = branches[e].tap != 0.0 ? branches[e].tap : 1.0;
+        const double ang = M_PI / 180.0 * branches[e].shift;
+        const double tr = a * std::cos(ang), ti = a * std::sin(ang), t2 = tr * tr + ti * ti;
+        dy[4 * e + 0] = make_double2(1.0 / t2, 0.0);
+        dy[4 * e + 1] = make_double2(-tr / t2, -ti / t2);  // -1/conj(t) = -t/|t|^2
+        dy[4 * e + 2] = make_double2(-tr / t2, ti / t2);   // -1/t = -conj(t)/|t|^2
+        dy[4 * e + 3] = make_double2(1.0, 0.0);
+      }
+      upload(h->br_dy, dy);
       upload(h->br_y, by);
       std::vector<double2> sb(g.nb), v0(g.nb);
       for (int i = 0; i < g.nb; ++i) {
@@ -1133,6 +1220,62 @@ int32_t mpf_mismatch_noalloc(mpf_handle* h, const double* v, double* max_mis, vo
     CUDA_TRY(cudaGetLastError());
     k_acc_drain<<<(h->ncases + 255) / 256, 256, 0, st>>>(acc, max_mis, h->ncases);
     CUDA_TRY(cudaGetLastError());
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_set_ratings(mpf_handle* h, const double* rating) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (!rating) {
+      h->rating.release();
+      return MPF_OK;
+    }
+    std::vector<double> r(rating, rating + h->g.nbr);
+    for (double v : r)
+      if (!std::isfinite(v) || v < 0.0) return fail(h, MPF_ERR_BAD_INPUT, "ratings must be finite and >= 0");
+    CUDA_TRY(cudaStreamSynchronize(h->own_stream));
+    upload(h->rating, r);
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_branch_flows(mpf_handle* h, double* ploss, double* overload, double* sf, double* st, void* stream) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (!h->have_results) return fail(h, MPF_ERR_STATE, "no solved voltages: call mpf_solve first");
+  if (!ploss) return fail(h, MPF_ERR_BAD_INPUT, "ploss must be a device pointer");
+  if (overload && !h->rating.p) return fail(h, MPF_ERR_STATE, "overload needs ratings: call mpf_set_ratings");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st_ = stream ? (cudaStream_t)stream : h->own_stream;
+    CUDA_TRY(cudaStreamWaitEvent(st_, h->t1, 0));
+    CUDA_TRY(cudaMemsetAsync(ploss, 0, (size_t)h->ncases * sizeof(double), st_));
+    if (overload) CUDA_TRY(cudaMemsetAsync(overload, 0, (size_t)h->ncases * sizeof(double), st_));
+    const dim3 grid((unsigned)((h->g.nbr + 63) / 64), (unsigned)h->ngroups);
+    k_branch_flow<<<grid, 256, 0, st_>>>(h->dev(), h->g.nbr, h->ncases, overload ? h->rating.as<double>() : nullptr,
+                                         ploss, overload, reinterpret_cast<double2*>(sf), reinterpret_cast<double2*>(st));
+    CUDA_TRY(cudaGetLastError());
+    h->last_stream = st_;
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_adjoint(mpf_handle* h, int32_t precision, double* grad_p, double* grad_q, double* grad_g,
+                    double* grad_b, void* stream) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (!h->have_results) return fail(h, MPF_ERR_STATE, "no solved voltages: call mpf_solve first");
+  if (!h->rating.p) return fail(h, MPF_ERR_STATE, "the adjoint's loss needs ratings: call mpf_set_ratings");
+  if (precision != MPF_FP64 && precision != MPF_MIXED) return fail(h, MPF_ERR_BAD_INPUT, "unknown precision");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->own_stream;
+    CUDA_TRY(cudaStreamWaitEvent(st, h->t1, 0));
+    ensure_attrs<double>(h->device);
+    ensure_attrs<float>(h->device);
+    if (precision == MPF_FP64) adjoint_impl<double>(h, st, grad_p, grad_q, grad_g, grad_b);
+    else adjoint_impl<float>(h, st, grad_p, grad_q, grad_g, grad_b);
+    h->last_stream = st;
     return MPF_OK;
   });
 }

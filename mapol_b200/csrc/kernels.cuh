@@ -44,6 +44,7 @@ struct DevGrid {
   const double2* y_val;
   const int* y_diag;        // [nb] position of (i, i)
   const int4* br_ypos;      // per branch: Ybus positions (ff, ft, tf, tt)
+  const int2* br_ft;        // per branch: from, to buses
   const double2* br_y;      // per branch: 4 admittances
   const double2* sbus0;     // [nb]
   const double2* sbus_case; // [g][nb][32] or null
@@ -675,6 +676,264 @@ __global__ void k_acc_drain(unsigned long long* __restrict__ acc, double* __rest
   if (c >= n) return;
   out[c] = __longlong_as_double((long long)acc[c]);
   acc[c] = 0ull;
+}
+
+// ---------------------------------------------------------------- branch flows
+// Per case and branch: Sf = Vf conj(Yff Vf + Yft Vt), St = Vt conj(Ytf Vf + Ytt Vt)
+// (an outaged branch carries nothing).  Per case sums: active loss sum(Re Sf + Re St)
+// as mkl_computeLoss / hybrid_computeLoss + reduceLoss (runpf.h:228-257, 543-604),
+// and, with ratings, the overload loss sum(relu(|Sf| - 0.9 rating)^2).
+// Grid (branch blocks of 256, groups); thread = (branch, lane).
+__global__ void __launch_bounds__(256) k_branch_flow(DevGrid d, int nbr, int ncases, const double* __restrict__ rating,
+                                                     double* __restrict__ ploss, double* __restrict__ overload,
+                                                     double2* __restrict__ sf_out, double2* __restrict__ st_out) {
+  const int g = blockIdx.y;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = g * 32 + lane;
+  LaneOut o;
+  load_outages(d, c, o);
+  double lsum = 0.0, osum = 0.0;
+  const int k0 = blockIdx.x * 64;
+  const int k1 = min(nbr, k0 + 64);
+  for (int k = k0 + warp; k < k1; k += 8) {
+    bool out = false;
+#pragma unroll
+    for (int q = 0; q < kMaxOut; ++q) out |= (o.e[q] == k);
+    double2 sf = make_double2(0.0, 0.0), stt = make_double2(0.0, 0.0);
+    if (!out) {
+      const int2 ft = d.br_ft[k];
+      const double2* y = d.br_y + 4 * k;
+      const double2 vf = d.V[at32(g, d.nb, ft.x, lane)], vt = d.V[at32(g, d.nb, ft.y, lane)];
+      const double2 i_f = make_double2(y[0].x * vf.x - y[0].y * vf.y + y[1].x * vt.x - y[1].y * vt.y,
+                                       y[0].x * vf.y + y[0].y * vf.x + y[1].x * vt.y + y[1].y * vt.x);
+      const double2 i_t = make_double2(y[2].x * vf.x - y[2].y * vf.y + y[3].x * vt.x - y[3].y * vt.y,
+                                       y[2].x * vf.y + y[2].y * vf.x + y[3].x * vt.y + y[3].y * vt.x);
+      sf = make_double2(vf.x * i_f.x + vf.y * i_f.y, vf.y * i_f.x - vf.x * i_f.y);
+      stt = make_double2(vt.x * i_t.x + vt.y * i_t.y, vt.y * i_t.x - vt.x * i_t.y);
+    }
+    lsum += sf.x + stt.x;
+    if (rating) {
+      const double ex = sqrt(sf.x * sf.x + sf.y * sf.y) - 0.9 * rating[k];
+      if (ex > 0.0) osum += ex * ex;
+    }
+    if (c < ncases) {
+      if (sf_out) sf_out[(size_t)c * nbr + k] = sf;
+      if (st_out) st_out[(size_t)c * nbr + k] = stt;
+    }
+  }
+  __shared__ double red[2][8][32];
+  red[0][warp][lane] = lsum;
+  red[1][warp][lane] = osum;
+  __syncthreads();
+  if (warp == 0 && c < ncases) {
+    double a = 0.0, b = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      a += red[0][w][lane];
+      b += red[1][w][lane];
+    }
+    atomicAdd(&ploss[c], a);
+    if (overload) atomicAdd(&overload[c], b);
+  }
+}
+
+// ---------------------------------------------------------------- adjoint
+// Gradient of the per-case overload loss L = sum_k relu(|Sf_k| - 0.9 r_k)^2 w.r.t.
+// bus injections and branch series admittance g + jb, through J^T lambda = dL/dx
+// (x = [Va of PV/PQ buses, Vm of PQ buses], the Newton variables).
+//
+// With Sf = |Vf|^2 conj(Yff) + W, W = Vf conj(Yft Vt), E = |Sf| - 0.9 r > 0 and
+// c = 2E/|Sf|:  dL/dVa_f = -c Im(conj(Sf) W),  dL/dVa_t = +c Im(conj(Sf) W),
+//               dL/dVm_f = c Re(conj(Sf) (2|Vf| conj(Yff) + W/|Vf|)),
+//               dL/dVm_t = c Re(conj(Sf) W) / |Vt|.
+// Thread per (branch, lane), scattered into g (the right-hand side of J^T) with atomics.
+template <typename T>
+__global__ void __launch_bounds__(256) k_adj_dldx(DevGrid d, int nbr, const double* __restrict__ rating, T* __restrict__ g) {
+  const int grp = blockIdx.y;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = grp * 32 + lane;
+  if (d.status[c] != ST_CONVERGED) return;
+  LaneOut o;
+  load_outages(d, c, o);
+  const int k1 = min(nbr, (int)(blockIdx.x + 1) * 64);
+  for (int k = blockIdx.x * 64 + warp; k < k1; k += 8) {
+    bool out = false;
+#pragma unroll
+    for (int q = 0; q < kMaxOut; ++q) out |= (o.e[q] == k);
+    if (out) continue;
+    const int2 ft = d.br_ft[k];
+    const double2* y = d.br_y + 4 * k;
+    const double2 vf = d.V[at32(grp, d.nb, ft.x, lane)], vt = d.V[at32(grp, d.nb, ft.y, lane)];
+    // W = Vf conj(Yft Vt)
+    const double2 yv = make_double2(y[1].x * vt.x - y[1].y * vt.y, y[1].x * vt.y + y[1].y * vt.x);
+    const double2 W = make_double2(vf.x * yv.x + vf.y * yv.y, vf.y * yv.x - vf.x * yv.y);
+    const double mf2 = vf.x * vf.x + vf.y * vf.y;
+    const double2 S = make_double2(mf2 * y[0].x + W.x, -mf2 * y[0].y + W.y);
+    const double aS = sqrt(S.x * S.x + S.y * S.y);
+    const double E = aS - 0.9 * rating[k];
+    if (!(E > 0.0)) continue;
+    const double cc = 2.0 * E / aS;
+    // conj(S) W
+    const double swr = S.x * W.x + S.y * W.y, swi = S.x * W.y - S.y * W.x;
+    const double mf = sqrt(mf2), mt = sqrt(vt.x * vt.x + vt.y * vt.y);
+    // conj(S) (2|Vf| conj(Yff) + W/|Vf|), real part
+    const double dvm_f = cc * (2.0 * mf * (S.x * y[0].x - S.y * y[0].y) + swr / mf);
+    const int2 vfv = d.jvar[ft.x], vtv = d.jvar[ft.y];
+    if (vfv.x >= 0) atomicAdd(&g[at32(grp, d.n_jac, vfv.x, lane)], (T)(-cc * swi));
+    if (vtv.x >= 0) atomicAdd(&g[at32(grp, d.n_jac, vtv.x, lane)], (T)(cc * swi));
+    if (vfv.y >= 0) atomicAdd(&g[at32(grp, d.n_jac, vfv.y, lane)], (T)dvm_f);
+    if (vtv.y >= 0) atomicAdd(&g[at32(grp, d.n_jac, vtv.y, lane)], (T)(cc * swr / mt));
+  }
+}
+
+// U^T z = g, supernodes bottom-up (thread per case, warp per (supernode, group)):
+// pivots in order, each pushes U(p, i) z_p into the later rows of its front; the
+// non-pivot rows travel to the parent as a carried vector (as k_mf_fsolve).
+template <typename T>
+__global__ void __launch_bounds__(128) k_mf_fsolve_t(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+                                                     int ngroups, int fcap, const T* __restrict__ pan,
+                                                     T* __restrict__ cbr, T* __restrict__ x,
+                                                     const int* __restrict__ group_active) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  T* b = reinterpret_cast<T*>(smem_raw) + (size_t)warp * fcap * 32;
+  const long long ntasks = (long long)nsn_l * ngroups;
+  for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
+    const int s = task_sn[t / ngroups];
+    const int g = (int)(t % ngroups);
+    if (!group_active[g]) continue;
+    const int w = L.sn_w[s], f = L.sn_f[s];
+    const int* rows = L.sn_rows + L.sn_rptr[s];
+    for (int i = 0; i < f; ++i) b[i * 32 + lane] = (T)0;
+    for (int p = 0; p < w; ++p) b[p * 32 + lane] = x[at32(g, L.n, rows[p], lane)];
+    for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
+      const int ch = L.child_list[ci];
+      const int m = L.sn_f[ch] - L.sn_w[ch];
+      const int* rel = L.relmap + L.rel_ptr[ch];
+      for (int a = 0; a < m; ++a) b[rel[a] * 32 + lane] += cbr[at32(g, L.sumcbr, L.cbr_off[ch] + a, lane)];
+    }
+    const long long po = L.pan_off[s];
+    for (int p = 0; p < w; ++p) {
+      const T* urow = pan + at32(g, L.nnz, po + (long long)p * f, lane);
+      const T zp = b[p * 32 + lane] / urow[(size_t)p * 32];
+      b[p * 32 + lane] = zp;
+      for (int i = p + 1; i < f; ++i) b[i * 32 + lane] -= urow[(size_t)i * 32] * zp;
+    }
+    for (int p = 0; p < w; ++p) x[at32(g, L.n, rows[p], lane)] = b[p * 32 + lane];
+    if (L.sn_parent[s] >= 0)
+      for (int a = 0; a < f - w; ++a) cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = b[(w + a) * 32 + lane];
+    __syncwarp();
+  }
+}
+
+// L^T lambda = z, supernodes top-down (thread per case): the ancestors' lambda are
+// final; lambda_p = z_p - sum_{i > p} L(i, p) lambda_i (unit diagonal), with L(i, p)
+// in the U-panel below the diagonal block's diagonal (i < w) or in the L-panel.
+template <typename T>
+__global__ void __launch_bounds__(128) k_mf_bsolve_t(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+                                                     int ngroups, int fcap, const T* __restrict__ pan,
+                                                     T* __restrict__ x, const int* __restrict__ group_active) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  T* xs = reinterpret_cast<T*>(smem_raw) + (size_t)warp * fcap * 32;
+  const long long ntasks = (long long)nsn_l * ngroups;
+  for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
+    const int s = task_sn[t / ngroups];
+    const int g = (int)(t % ngroups);
+    if (!group_active[g]) continue;
+    const int w = L.sn_w[s], f = L.sn_f[s];
+    const int* rows = L.sn_rows + L.sn_rptr[s];
+    const long long po = L.pan_off[s];
+    for (int q = 0; q < f; ++q) xs[q * 32 + lane] = x[at32(g, L.n, rows[q], lane)];
+    for (int p = w - 1; p >= 0; --p) {
+      T acc = xs[p * 32 + lane];
+      for (int i = p + 1; i < w; ++i) acc -= pan[at32(g, L.nnz, po + (long long)i * f + p, lane)] * xs[i * 32 + lane];
+      for (int i = w; i < f; ++i)
+        acc -= pan[at32(g, L.nnz, po + (long long)w * f + (long long)(i - w) * w + p, lane)] * xs[i * 32 + lane];
+      xs[p * 32 + lane] = acc;
+    }
+    for (int p = 0; p < w; ++p) x[at32(g, L.n, rows[p], lane)] = xs[p * 32 + lane];
+    __syncwarp();
+  }
+}
+
+// dL/dP_i = lambda(P_i row), dL/dQ_i = lambda(Q_i row): F = S(V) - Sbus, so
+// dF/dSbus = -I and dL/dtheta = dL/dtheta|explicit - lambda^T dF/dtheta.
+template <typename T>
+__global__ void k_adj_grad_bus(DevGrid d, int ncases, const T* __restrict__ lam, double* __restrict__ gp,
+                               double* __restrict__ gq) {
+  const size_t total = (size_t)ncases * d.nb;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t / d.nb), i = (int)(t % d.nb);
+    const int2 jv = d.jvar[i];
+    const bool ok = d.status[c] == ST_CONVERGED;
+    if (gp) gp[t] = (ok && jv.x >= 0) ? (double)lam[at32(c >> 5, d.n_jac, jv.x, c & 31)] : 0.0;
+    if (gq) gq[t] = (ok && jv.y >= 0) ? (double)lam[at32(c >> 5, d.n_jac, jv.y, c & 31)] : 0.0;
+  }
+}
+
+// Branch series admittance y = g + jb.  dY/dg for (ff, ft, tf, tt) = a = (1/|t|^2,
+// -1/conj(t), -1/t, 1) (br_dy), dY/db = j a.  With Df = Vf conj(a_ff Vf + a_ft Vt),
+// Dt = Vt conj(a_tf Vf + a_tt Vt) (the branch's injections' derivative w.r.t. g):
+//   dL/dg = c Re(conj(Sf) Df) - [lam_Pf Re Df + lam_Qf Im Df + lam_Pt Re Dt + lam_Qt Im Dt]
+//   dL/db = c Im(conj(Sf) Df) - [lam_Pf Im Df - lam_Qf Re Df + lam_Pt Im Dt - lam_Qt Re Dt]
+// (first terms only when the branch is overloaded).  Thread per (branch, lane).
+template <typename T>
+__global__ void __launch_bounds__(256) k_adj_grad_branch(DevGrid d, int nbr, int ncases, const double* __restrict__ rating,
+                                                         const double2* __restrict__ br_dy, const T* __restrict__ lam,
+                                                         double* __restrict__ gg, double* __restrict__ gb) {
+  const int grp = blockIdx.y;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = grp * 32 + lane;
+  LaneOut o;
+  load_outages(d, c, o);
+  const bool ok = c < ncases && d.status[c] == ST_CONVERGED;
+  const int k1 = min(nbr, (int)(blockIdx.x + 1) * 64);
+  for (int k = blockIdx.x * 64 + warp; k < k1; k += 8) {
+    if (c >= ncases) continue;
+    bool out = false;
+#pragma unroll
+    for (int q = 0; q < kMaxOut; ++q) out |= (o.e[q] == k);
+    double rg = 0.0, rb = 0.0;
+    if (ok && !out) {
+      const int2 ft = d.br_ft[k];
+      const double2* y = d.br_y + 4 * k;
+      const double2* a = br_dy + 4 * k;
+      const double2 vf = d.V[at32(grp, d.nb, ft.x, lane)], vt = d.V[at32(grp, d.nb, ft.y, lane)];
+      // Df = Vf conj(a_ff Vf + a_ft Vt), Dt = Vt conj(a_tf Vf + a_tt Vt)
+      const double2 u = make_double2(a[0].x * vf.x - a[0].y * vf.y + a[1].x * vt.x - a[1].y * vt.y,
+                                     a[0].x * vf.y + a[0].y * vf.x + a[1].x * vt.y + a[1].y * vt.x);
+      const double2 Df = make_double2(vf.x * u.x + vf.y * u.y, vf.y * u.x - vf.x * u.y);
+      const double2 u2 = make_double2(a[2].x * vf.x - a[2].y * vf.y + a[3].x * vt.x - a[3].y * vt.y,
+                                      a[2].x * vf.y + a[2].y * vf.x + a[3].x * vt.y + a[3].y * vt.x);
+      const double2 Dt = make_double2(vt.x * u2.x + vt.y * u2.y, vt.y * u2.x - vt.x * u2.y);
+      // explicit part through this branch's own Sf
+      const double2 yv = make_double2(y[0].x * vf.x - y[0].y * vf.y + y[1].x * vt.x - y[1].y * vt.y,
+                                      y[0].x * vf.y + y[0].y * vf.x + y[1].x * vt.y + y[1].y * vt.x);
+      const double2 S = make_double2(vf.x * yv.x + vf.y * yv.y, vf.y * yv.x - vf.x * yv.y);
+      const double aS = sqrt(S.x * S.x + S.y * S.y);
+      const double E = aS - 0.9 * rating[k];
+      if (E > 0.0) {
+        const double cc = 2.0 * E / aS;
+        rg += cc * (S.x * Df.x + S.y * Df.y);
+        rb += cc * (S.x * Df.y - S.y * Df.x);
+      }
+      const int2 vfv = d.jvar[ft.x], vtv = d.jvar[ft.y];
+      const double lPf = vfv.x >= 0 ? (double)lam[at32(grp, d.n_jac, vfv.x, lane)] : 0.0;
+      const double lQf = vfv.y >= 0 ? (double)lam[at32(grp, d.n_jac, vfv.y, lane)] : 0.0;
+      const double lPt = vtv.x >= 0 ? (double)lam[at32(grp, d.n_jac, vtv.x, lane)] : 0.0;
+      const double lQt = vtv.y >= 0 ? (double)lam[at32(grp, d.n_jac, vtv.y, lane)] : 0.0;
+      rg -= lPf * Df.x + lQf * Df.y + lPt * Dt.x + lQt * Dt.y;
+      rb -= lPf * Df.y - lQf * Df.x + lPt * Dt.y - lQt * Dt.x;
+    }
+    if (gg) gg[(size_t)c * nbr + k] = rg;
+    if (gb) gb[(size_t)c * nbr + k] = rb;
+  }
+}
+
+__global__ void k_fill_int(int* p, int n, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
 }
 
 // ---------------------------------------------------------------- results

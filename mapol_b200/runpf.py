@@ -56,6 +56,7 @@ class PowerFlow:
         rc = lib().mpf_create(ptr(self.buses), len(self.buses), ptr(self.branches), len(self.branches),
                               ctypes.byref(opt), ctypes.byref(h))
         self._h = h
+        self.device = device
         if rc != 0:
             msg = lib().mpf_last_error(h).decode() if h.value else lib().mpf_status_string(rc).decode()
             if h.value:
@@ -120,6 +121,56 @@ class PowerFlow:
                                          ptr(v), ptr(it), ptr(st), ptr(mm)))
         self.n_cases = n
         return Results(v[..., 0] + 1j * v[..., 1], it, st, mm)
+
+    def set_ratings(self, rating):
+        """Branch ratings (p.u. apparent power, [n_branch]) for the overload loss."""
+        r = None if rating is None else np.ascontiguousarray(rating, dtype=np.float64)
+        self._check(lib().mpf_set_ratings(self._h, ptr(r)))
+        self.has_ratings = r is not None
+
+    def branch_flows(self, flows=False):
+        """Per-case active loss (and overload loss when ratings are set) at the solved
+        voltages; with flows=True also Sf, St (n_cases, n_branch) complex."""
+        import torch
+
+        n, nbr = self.n_cases, len(self.branches)
+        dev = torch.device("cuda", self.device)
+        ploss = torch.zeros(n, dtype=torch.float64, device=dev)
+        over = torch.zeros(n, dtype=torch.float64, device=dev) if getattr(self, "has_ratings", False) else None
+        sf = torch.zeros((n, nbr, 2), dtype=torch.float64, device=dev) if flows else None
+        st = torch.zeros((n, nbr, 2), dtype=torch.float64, device=dev) if flows else None
+        dp = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        self._check(lib().mpf_branch_flows(self._h, dp(ploss), dp(over), dp(sf), dp(st), None))
+        torch.cuda.synchronize(dev)
+        out = {"ploss": ploss.cpu().numpy()}
+        if over is not None:
+            out["overload"] = over.cpu().numpy()
+        if flows:
+            a, b = sf.cpu().numpy(), st.cpu().numpy()
+            out["sf"] = a[..., 0] + 1j * a[..., 1]
+            out["st"] = b[..., 0] + 1j * b[..., 1]
+        return out
+
+    def adjoint(self, precision=FP64):
+        """Gradients of each converged case's overload loss (ratings must be set):
+        dict of (n_cases, n_bus) grad_p, grad_q and (n_cases, n_branch) grad_g, grad_b."""
+        import torch
+
+        n, nb, nbr = self.n_cases, len(self.buses), len(self.branches)
+        dev = torch.device("cuda", self.device)
+        bufs = {"grad_p": (n, nb), "grad_q": (n, nb), "grad_g": (n, nbr), "grad_b": (n, nbr)}
+        t = {k: torch.zeros(v, dtype=torch.float64, device=dev) for k, v in bufs.items()}
+        self._check(lib().mpf_adjoint(self._h, precision, t["grad_p"].data_ptr(), t["grad_q"].data_ptr(),
+                                      t["grad_g"].data_ptr(), t["grad_b"].data_ptr(), None))
+        torch.cuda.synchronize(dev)
+        return {k: v.cpu().numpy() for k, v in t.items()}
+
+    def fitness(self, results=None):
+        """The reference's per-case fitness after hybrid_runpf: total active loss when
+        the case converged, DBL_MAX otherwise (runpf.h:748-791)."""
+        res = results if results is not None else self.results()
+        loss = self.branch_flows()["ploss"]
+        return np.where(res.status == T.CASE_CONVERGED, loss, np.finfo(np.float64).max)
 
     def timing(self):
         t = T.Timing()

@@ -236,3 +236,29 @@ def test_graph_and_direct_launches_agree(gpu):
     for (va, ia), (vb, ib) in zip(out[0], out[1]):
         assert np.array_equal(ia, ib)
         assert np.array_equal(va, vb)
+
+
+def test_branch_flows_loss_and_overload_match_oracle(gpu):
+    buses, branches, cases = m.workload("cfg1_300bus")
+    cases = cases[:40] + [[]]
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.FP64)
+        res = pf.results()
+        fl = pf.branch_flows(flows=True)
+        rating = 1.2 * np.abs(fl["sf"][-1])  # base case flows
+        pf.set_ratings(rating)
+        fl2 = pf.branch_flows()
+        fit = pf.fitness(res)
+    np.testing.assert_allclose(fl["ploss"], fl2["ploss"], rtol=1e-12, atol=0)
+    for k in (0, 5, 17, 40):
+        ref = oracle.loss(buses, branches, res.v[k], cases[k])
+        assert abs(fl["ploss"][k] - ref) <= 1e-10 * max(1.0, abs(ref))
+    # overload from the flows themselves, and outaged branches carry nothing
+    ex = np.maximum(np.abs(fl["sf"]) - 0.9 * rating, 0.0)
+    np.testing.assert_allclose(fl2["overload"], (ex ** 2).sum(1), rtol=1e-10, atol=1e-14)
+    for k in range(40):
+        assert fl["sf"][k, cases[k][0]] == 0 and fl["st"][k, cases[k][0]] == 0
+    assert (fl2["overload"][:40] > 0).any()
+    # per-case sums are accumulated with atomics: equal up to summation order
+    np.testing.assert_allclose(fit, fl["ploss"], rtol=1e-12, atol=0)
