@@ -262,3 +262,23 @@ def test_branch_flows_loss_and_overload_match_oracle(gpu):
     assert (fl2["overload"][:40] > 0).any()
     # per-case sums are accumulated with atomics: equal up to summation order
     np.testing.assert_allclose(fit, fl["ploss"], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("name", ["case118", "case300"])
+def test_real_matpower_grids_n1_match_oracle(gpu, name):
+    """The reference's bundled IEEE 118 / 300-bus cases (fixture converted from its
+    datasets), base + 40 N-1 outages, solved from the stored start point."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "matpower_cases.npz"))
+    buses, branches = g[name + "_buses"], g[name + "_branches"]
+    cases = m.n1_cases(branches, len(buses), 40, 3, with_base=True)
+    ref = _oracle(buses, branches, cases, m.NR)
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.FP64)
+        res = pf.results()
+        pf.solve(m.NR, m.MIXED)
+        res32 = pf.results()
+    _compare(res, ref)
+    _compare(res32, ref, max_extra_iter=1)
