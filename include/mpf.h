@@ -164,6 +164,29 @@ int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases,
                       const int32_t* outage_offsets, const int32_t* outage_branches,
                       const double* sbus);
 
+/* Per-case control overrides: the optimiser's structures of
+ * src/pso/Particula.h:26-60 (kinds keep the values of its enum Tipo), applied as
+ * hybrid_computeVoltage (src/powerflow/runpf.h:524-541) and hybrid_computeYfYt
+ * (src/powerflow/makeYbus.h:313-332) apply a particle:
+ *   MPF_CTRL_AVR  index = PV or slack bus;      value = its |V| set-point (p.u.)
+ *   MPF_CTRL_OLTC index = branch with tap != 0; value = its tap ratio (> 0)
+ *   MPF_CTRL_SHC  index = bus;                  value = its shunt susceptance Bsh (p.u.)
+ * values[c * n_controls + k] is control k's value in case c.  Replaces
+ * hybrid_runpf's particle upload (runpf.h:606-624).  A tap or shunt change enters
+ * the case's Ybus and B''; B' ignores both, as the reference builds it from zeroed
+ * taps and shunts (makeB.h:311-324).  A tap control on a branch that the case
+ * outages has no effect.  Must follow mpf_set_cases, which clears the controls;
+ * n_controls = 0 clears them.  Each (kind, index) at most once. */
+#define MPF_CTRL_AVR  1
+#define MPF_CTRL_OLTC 2
+#define MPF_CTRL_SHC  3
+typedef struct mpf_control {
+  int32_t kind;
+  int32_t index;
+} mpf_control;
+int32_t mpf_set_controls(mpf_handle* h, int32_t n_controls, const mpf_control* controls,
+                         const double* values);
+
 /* ---- solve (replaces hybrid_runpf) ------------------------------------- */
 /* Runs alg (MPF_NR / MPF_FDXB / MPF_FDBX) at precision (MPF_FP64 / MPF_MIXED) over
  * every case, from the reference's start point (runpf.h:211-226: V = vm e^{j va},

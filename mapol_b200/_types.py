@@ -45,6 +45,9 @@ FP64, MIXED = 0, 1
 MAX_IT_NR, MAX_IT_FD, EPS = 10, 30, 1e-8
 
 CASE_RUNNING, CASE_CONVERGED, CASE_MAX_ITER, CASE_DIVERGED, CASE_SINGULAR = 0, 1, 2, 3, 4
+# per-case control kinds (the values of Particula::Estrutura::Tipo, src/pso/Particula.h:27-29)
+CTRL_AVR, CTRL_OLTC, CTRL_SHC = 1, 2, 3
+CONTROL_DTYPE = np.dtype([("kind", "<i4"), ("index", "<i4")])
 
 
 class SynthParams(ctypes.Structure):

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -408,6 +409,21 @@ struct mpf_handle {
   DevBuf eval_acc;  // mpf_mismatch accumulator, allocated on first use
   DevBuf br_dy;     // per branch dY/dg for (ff, ft, tf, tt), adjoint
   DevBuf adj_status;  // statuses the adjoint's refactorisation may write (kept apart)
+  std::vector<mpf_bus> buses;        // the grid as given (controls read base values)
+  std::vector<mpf_branch> branches;
+  // per-case controls of the current cases (mpf_set_controls)
+  struct Controls {
+    int nc = 0, navr = 0, noltc = 0, nshc = 0, nslot = 0;
+    DevBuf val, avr, oltc, oltc_par, shc, shc_base, slot_ptr, slot_ent, y_slot, br_ctl, dy, bry, bdy, fdpos[2];
+    void clear() { nc = navr = noltc = nshc = nslot = 0; }
+    size_t bytes() const {
+      const DevBuf* all[] = {&val, &avr, &oltc, &oltc_par, &shc, &shc_base, &slot_ptr, &slot_ent,
+                             &y_slot, &br_ctl, &dy, &bry, &bdy, &fdpos[0], &fdpos[1]};
+      size_t b = 0;
+      for (auto p : all) b += p->bytes;
+      return b;
+    }
+  } ctl;
   bool have_cases = false, have_results = false;
   int last_alg = -1, last_prec = -1;
   cudaStream_t last_stream = nullptr;  // stream of the last solve / result copy
@@ -419,6 +435,7 @@ struct mpf_handle {
     cudaGraph_t graph[4] = {};
     cudaGraphExec_t exec[4] = {};
     const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
+    DevGrid dkey;  // the grid descriptor the kernels were captured with
     int ngroups = 0, launches[4] = {0, 0, 0, 0};
     void release() {
       for (int k = 0; k < 4; ++k) {
@@ -434,6 +451,7 @@ struct mpf_handle {
 
   DevGrid dev() const {
     DevGrid d;
+    std::memset(&d, 0, sizeof(d));  // byte-comparable (graph key)
     d.nb = g.nb;
     d.nfree = (int)g.mis_rows.size();
     d.ngroups = ngroups;
@@ -463,7 +481,39 @@ struct mpf_handle {
     d.group_active = group_active.as<int>();
     d.any_active = any_active.as<int>();
     d.it_ptr = it_ctr.as<int>();
+    if (ctl.nc > 0) {
+      d.nslot = ctl.nslot;
+      d.noltc = ctl.noltc;
+      if (ctl.nslot > 0) {
+        d.y_slot = ctl.y_slot.as<int>();
+        d.ctl_dy = ctl.dy.as<double2>();
+      }
+      if (ctl.noltc > 0) {
+        d.br_ctl = ctl.br_ctl.as<int>();
+        d.ctl_bry = ctl.bry.as<double2>();
+        d.ctl_bdy = ctl.bdy.as<double2>();
+      }
+    }
     return d;
+  }
+
+  DevCtl devctl() const {
+    DevCtl t;
+    std::memset(&t, 0, sizeof(t));
+    t.nc = ctl.nc;
+    t.navr = ctl.navr;
+    t.noltc = ctl.noltc;
+    t.nshc = ctl.nshc;
+    t.nslot = ctl.nslot;
+    t.val = ctl.val.as<double>();
+    t.avr = ctl.avr.as<int2>();
+    t.oltc = ctl.oltc.as<int2>();
+    t.oltc_par = ctl.oltc_par.as<double>();
+    t.shc = ctl.shc.as<int2>();
+    t.shc_base = ctl.shc_base.as<double>();
+    t.slot_ptr = ctl.slot_ptr.as<int>();
+    t.slot_ent = ctl.slot_ent.as<int2>();
+    return t;
   }
 
   size_t device_bytes() const {
@@ -473,6 +523,7 @@ struct mpf_handle {
                            &any_active, &vout, &small_out, &fdvar, &eval_acc, &it_ctr, &br_dy,
                            &adj_status};
     for (auto p : all) b += p->bytes;
+    b += ctl.bytes();
     const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
     for (auto s : systems) {
       for (int p = 0; p < 2; ++p) b += s->A[p].bytes + s->pan[p].bytes + s->cb[p].bytes + s->cbr[p].bytes + s->x[p].bytes;
@@ -543,6 +594,27 @@ bool any_active(mpf_handle* h, cudaStream_t st) {
   return *h->h_any != 0;
 }
 
+// Newton mismatch (with the Jacobian when jac), in its variant with or without
+// per-case Ybus controls
+template <typename T>
+void launch_mismatch_nr(const DevGrid& d, dim3 rg, cudaStream_t st, T* x, T* A, bool jac) {
+  const bool ctl = d.y_slot != nullptr;
+  if (jac && ctl) k_mismatch_nr<T, true, true><<<rg, 256, 0, st>>>(d, x, A);
+  else if (jac) k_mismatch_nr<T, true, false><<<rg, 256, 0, st>>>(d, x, A);
+  else if (ctl) k_mismatch_nr<T, false, true><<<rg, 256, 0, st>>>(d, x, A);
+  else k_mismatch_nr<T, false, false><<<rg, 256, 0, st>>>(d, x, A);
+  CUDA_TRY(cudaGetLastError());
+}
+
+// AVR controls: the set-points of the current cases into V (after k_init)
+int apply_avr(mpf_handle* h, cudaStream_t st) {
+  if (h->ctl.nc == 0 || h->ctl.navr == 0) return 0;
+  const size_t tot = (size_t)h->ngroups * h->ctl.navr * 32;
+  k_ctl_vm<<<(unsigned)std::min<size_t>(148 * 8, tot / 256 + 1), 256, 0, st>>>(h->dev(), h->devctl());
+  CUDA_TRY(cudaGetLastError());
+  return 1;
+}
+
 void check(mpf_handle* h, cudaStream_t st, int it, int max_it, int* nl) {
   CUDA_TRY(cudaMemsetAsync(h->any_active.p, 0, sizeof(int), st));
   const int nl_lanes = h->ngroups * 32;
@@ -571,8 +643,7 @@ int enqueue_nr_part(mpf_handle* h, int part, cudaStream_t st, T* A, T* pan, T* c
     CUDA_TRY(cudaGetLastError());
     ++nl;
   } else {
-    k_mismatch_nr<T, true><<<rg, 256, 0, st>>>(d, x, A);
-    CUDA_TRY(cudaGetLastError());
+    launch_mismatch_nr<T>(d, rg, st, x, A, true);
     CUDA_TRY(cudaMemsetAsync(h->any_active.p, 0, sizeof(int), st));
     const int nl_lanes = h->ngroups * 32;
     k_check<<<(nl_lanes + 255) / 256, 256, 0, st>>>(d, -1, h->opt.max_it_nr, h->opt.tol);
@@ -600,12 +671,11 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
   k_init<<<std::min(148 * 8, (int)((size_t)h->ngroups * h->g.nb * 32 / 256 + 1)), 256, 0, st>>>(d, h->ncases);
   CUDA_TRY(cudaGetLastError());
   ++nl;
+  nl += apply_avr(h, st);
   tm.end(ev);
   const int max_it = h->opt.max_it_nr;
   ev = tm.begin(FAM_MIS);
-  if (max_it > 0) k_mismatch_nr<T, true><<<rg, 256, 0, st>>>(d, x, A);
-  else k_mismatch_nr<T, false><<<rg, 256, 0, st>>>(d, x, A);
-  CUDA_TRY(cudaGetLastError());
+  launch_mismatch_nr<T>(d, rg, st, x, A, max_it > 0);
   ++nl;
   tm.end(ev);
   ev = tm.begin(FAM_OTHER);
@@ -615,8 +685,12 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
   int it = 0;
   auto& gph = h->nr_graph[P];
   if (h->opt.use_graph) {
+    // the captured kernels hold every device pointer of d by value: capture again
+    // when any of them (or the LU buffers) changed since
     const void* key[4] = {A, pan, cb, x};
-    if (gph.exec[0] && (gph.ngroups != h->ngroups || std::memcmp(gph.key, key, sizeof(key)) != 0)) gph.release();
+    if (gph.exec[0] && (gph.ngroups != h->ngroups || std::memcmp(gph.key, key, sizeof(key)) != 0 ||
+                        std::memcmp(&gph.dkey, &d, sizeof(d)) != 0))
+      gph.release();
     if (!gph.exec[0]) {
       // capture each part on a private stream (the caller's may be the legacy one)
       cudaStream_t cs;
@@ -629,6 +703,7 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
       }
       CUDA_TRY(cudaStreamDestroy(cs));
       std::memcpy(gph.key, key, sizeof(key));
+      std::memcpy(&gph.dkey, &d, sizeof(d));
       gph.ngroups = h->ngroups;
     }
   }
@@ -670,6 +745,7 @@ void solve_fd(mpf_handle* h, cudaStream_t st, int variant) {
   k_init<<<std::min(148 * 8, (int)((size_t)h->ngroups * h->g.nb * 32 / 256 + 1)), 256, 0, st>>>(d, h->ncases);
   CUDA_TRY(cudaGetLastError());
   ++nl;
+  nl += apply_avr(h, st);
   tm.end(ev);
   // B' and B'' of every case, factorised once and reused by all iterations
   ev = tm.begin(FAM_JAC);
@@ -685,6 +761,13 @@ void solve_fd(mpf_handle* h, cudaStream_t st, int variant) {
                                                                     fds[k]->br_bval.as<double4>(), S.A[P].as<T>());
     CUDA_TRY(cudaGetLastError());
     nl += 2;
+    if (k == 1 && h->ctl.nc > 0 && h->ctl.nslot > 0) {
+      const size_t tot = (size_t)h->ngroups * h->ctl.nslot * 32;
+      k_fd_ctl<T><<<(unsigned)std::min<size_t>(148 * 8, tot / 256 + 1), 256, 0, st>>>(
+          d, h->devctl(), variant, S.nA, h->ctl.fdpos[variant].as<int>(), fds[k]->br_bval.as<double4>(), S.A[P].as<T>());
+      CUDA_TRY(cudaGetLastError());
+      ++nl;
+    }
   }
   tm.end(ev);
   ev = tm.begin(FAM_FACT);
@@ -811,8 +894,7 @@ void adjoint_impl(mpf_handle* h, cudaStream_t st, double* gp, double* gq, double
   k_fill_int<<<(h->ngroups + 255) / 256, 256, 0, st>>>(d.group_active, h->ngroups, 1);
   CUDA_TRY(cudaGetLastError());
   const dim3 rg = row_grid(h);
-  k_mismatch_nr<T, true><<<rg, 256, 0, st>>>(d, x, A);
-  CUDA_TRY(cudaGetLastError());
+  launch_mismatch_nr<T>(d, rg, st, x, A, true);
   int nl = 0;
   launch_factor<T>(J, h->ngroups, A, pan, J.cb[P].as<T>(), J.cbr[P].as<T>(), x, h->adj_status.as<int>(),
                    d.group_active, 0, st, &nl);
@@ -889,6 +971,8 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
     CUDA_TRY(cudaSetDevice(h->device));
     const std::string msg = build_symbolic(buses, n_bus, branches, n_branch, h->g);
     if (!msg.empty()) return fail(h.get(), MPF_ERR_BAD_INPUT, msg);
+    h->buses.assign(buses, buses + n_bus);
+    h->branches.assign(branches, branches + n_branch);
     const GridSymbolic& g = h->g;
     int maxf = g.jac.max_front;
     for (int v = 0; v < 2; ++v) maxf = std::max({maxf, g.bp[v].lu.max_front, g.bpp[v].lu.max_front});
@@ -1069,8 +1153,154 @@ int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases, const int32_t* outage_offs
     h->ncases = n_cases;
     h->ngroups = ngroups;
     h->maxk = maxk;
+    h->ctl.clear();
     h->have_cases = true;
     h->have_results = false;
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_set_controls(mpf_handle* h, int32_t n_controls, const mpf_control* controls, const double* values) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  if (!h->have_cases) return fail(h, MPF_ERR_STATE, "mpf_set_cases must be called before mpf_set_controls");
+  if (n_controls < 0) return fail(h, MPF_ERR_BAD_INPUT, "n_controls must be >= 0");
+  if (n_controls > 0 && (!controls || !values)) return fail(h, MPF_ERR_BAD_INPUT, "controls and values are required");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    // the control buffers are rewritten below: wait for work that may still read them
+    CUDA_TRY(cudaStreamSynchronize(h->own_stream));
+    if (h->last_stream) CUDA_TRY(cudaStreamSynchronize(h->last_stream));
+    auto& C = h->ctl;
+    C.clear();
+    h->have_results = false;
+    if (n_controls == 0) return MPF_OK;
+    const GridSymbolic& g = h->g;
+    const int nc = n_controls, ncases = h->ncases, lanes = h->ngroups * 32;
+    std::vector<int2> avr, oltc, shc;
+    std::vector<double> base(nc);
+    std::set<std::pair<int, int>> seen;
+    for (int k = 0; k < nc; ++k) {
+      const int kind = controls[k].kind, idx = controls[k].index;
+      const std::string who = "control " + std::to_string(k);
+      if (!seen.insert({kind, idx}).second) return fail(h, MPF_ERR_BAD_INPUT, who + " repeats a (kind, index)");
+      if (kind == MPF_CTRL_AVR || kind == MPF_CTRL_SHC) {
+        if (idx < 0 || idx >= g.nb) return fail(h, MPF_ERR_BAD_INPUT, who + ": bus index out of range");
+        if (kind == MPF_CTRL_AVR) {
+          if (g.bus_type[idx] != MPF_BUS_PV && g.bus_type[idx] != MPF_BUS_SLACK)
+            return fail(h, MPF_ERR_BAD_INPUT, who + ": AVR on a bus that is neither PV nor slack");
+          avr.push_back(make_int2(idx, k));
+          base[k] = h->buses[idx].vm;
+        } else {
+          shc.push_back(make_int2(idx, k));
+          base[k] = h->buses[idx].bsh;
+        }
+      } else if (kind == MPF_CTRL_OLTC) {
+        if (idx < 0 || idx >= g.nbr) return fail(h, MPF_ERR_BAD_INPUT, who + ": branch index out of range");
+        if (h->branches[idx].tap == 0.0)
+          return fail(h, MPF_ERR_BAD_INPUT, who + ": OLTC on a branch without a tap (tap 0)");
+        oltc.push_back(make_int2(idx, k));
+        base[k] = h->branches[idx].tap;
+      } else {
+        return fail(h, MPF_ERR_BAD_INPUT, who + ": unknown kind");
+      }
+    }
+    // values, lane-interleaved; padding lanes hold the base values
+    std::vector<double> val((size_t)h->ngroups * nc * 32);
+    for (int c = 0; c < lanes; ++c)
+      for (int k = 0; k < nc; ++k) {
+        const double v = c < ncases ? values[(size_t)c * nc + k] : base[k];
+        if (!std::isfinite(v)) return fail(h, MPF_ERR_BAD_INPUT, "control values must be finite");
+        if (controls[k].kind != MPF_CTRL_SHC && !(v > 0.0))
+          return fail(h, MPF_ERR_BAD_INPUT, "AVR and OLTC values must be > 0");
+        val[((size_t)(c >> 5) * nc + k) * 32 + (c & 31)] = v;
+      }
+    // tap parameters: Ys, b/2, cos / sin of the shift, Ys with r = 0 (BX's B'')
+    std::vector<double> par(8 * oltc.size(), 0.0);
+    std::vector<int> br_ctl(g.nbr, -1);
+    for (size_t j = 0; j < oltc.size(); ++j) {
+      const mpf_branch& b = h->branches[oltc[j].x];
+      br_ctl[oltc[j].x] = (int)j;
+      if (!b.status) continue;
+      const double den = b.r * b.r + b.x * b.x;
+      const double ang = M_PI / 180.0 * b.shift;
+      double* p = &par[8 * j];
+      p[0] = b.r / den;
+      p[1] = -b.x / den;
+      p[2] = 0.5 * b.b;
+      p[3] = std::cos(ang);
+      p[4] = std::sin(ang);
+      p[5] = 0.0;
+      p[6] = -1.0 / b.x;
+    }
+    // slots: the distinct Ybus positions the taps (ff, ft, tf) and shunts (ii) change
+    std::vector<int> y_slot(g.y_col.size(), -1), slot_pos;
+    std::vector<std::vector<int2>> ents;
+    auto slot_of = [&](int p) {
+      if (y_slot[p] < 0) {
+        y_slot[p] = (int)slot_pos.size();
+        slot_pos.push_back(p);
+        ents.emplace_back();
+      }
+      return y_slot[p];
+    };
+    for (size_t j = 0; j < oltc.size(); ++j)
+      for (int q = 0; q < 3; ++q) ents[slot_of(g.br_pos[4 * oltc[j].x + q])].push_back(make_int2(q, (int)j));
+    for (size_t j = 0; j < shc.size(); ++j) ents[slot_of(g.y_diag[shc[j].x])].push_back(make_int2(3, (int)j));
+    std::vector<int> slot_ptr(1, 0);
+    std::vector<int2> slot_ent;
+    for (auto& e : ents) {
+      slot_ent.insert(slot_ent.end(), e.begin(), e.end());
+      slot_ptr.push_back((int)slot_ent.size());
+    }
+    // B'' array position of each slot, per fast-decoupled variant
+    std::vector<int> fdpos[2];
+    for (int v = 0; v < 2; ++v) {
+      const auto& fs = g.bpp[v];
+      fdpos[v].assign(slot_pos.size(), -1);
+      for (size_t s = 0; s < slot_pos.size(); ++s) {
+        const int2 e = ents[s][0];
+        fdpos[v][s] = e.x < 3 ? fs.br_pos[4 * oltc[e.y].x + e.x] : fs.diag_pos[shc[e.y].x];
+      }
+    }
+    std::vector<double> shc_base(shc.size());
+    for (size_t j = 0; j < shc.size(); ++j) shc_base[j] = h->buses[shc[j].x].bsh;
+    upload(C.val, val);
+    upload(C.avr, avr);
+    upload(C.oltc, oltc);
+    upload(C.oltc_par, par);
+    upload(C.shc, shc);
+    upload(C.shc_base, shc_base);
+    upload(C.slot_ptr, slot_ptr);
+    upload(C.slot_ent, slot_ent);
+    upload(C.y_slot, y_slot);
+    upload(C.br_ctl, br_ctl);
+    upload(C.fdpos[0], fdpos[0]);
+    upload(C.fdpos[1], fdpos[1]);
+    const size_t nbry = (size_t)h->ngroups * 4 * std::max<size_t>(oltc.size(), 1) * 32 * sizeof(double2);
+    if (!C.bry.p || C.bry.bytes < nbry) C.bry.alloc(nbry);
+    if (!C.bdy.p || C.bdy.bytes < nbry) C.bdy.alloc(nbry);
+    const size_t ndy = (size_t)h->ngroups * std::max<size_t>(slot_pos.size(), 1) * 32 * sizeof(double2);
+    if (!C.dy.p || C.dy.bytes < ndy) C.dy.alloc(ndy);
+    C.nc = nc;
+    C.navr = (int)avr.size();
+    C.noltc = (int)oltc.size();
+    C.nshc = (int)shc.size();
+    C.nslot = (int)slot_pos.size();
+    cudaStream_t st = h->own_stream;
+    const DevCtl t = h->devctl();
+    if (C.noltc > 0) {
+      const size_t tot = (size_t)h->ngroups * C.noltc * 32;
+      k_ctl_branch<<<(unsigned)std::min<size_t>(148 * 8, tot / 256 + 1), 256, 0, st>>>(t, h->ngroups, C.bry.as<double2>(),
+                                                                                       C.bdy.as<double2>());
+      CUDA_TRY(cudaGetLastError());
+    }
+    if (C.nslot > 0) {
+      const size_t tot = (size_t)h->ngroups * C.nslot * 32;
+      k_ctl_ydelta<<<(unsigned)std::min<size_t>(148 * 8, tot / 256 + 1), 256, 0, st>>>(h->dev(), t, C.bry.as<double2>(),
+                                                                                       C.dy.as<double2>());
+      CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
     return MPF_OK;
   });
 }

@@ -138,6 +138,7 @@ struct GridSymbolic {
     std::vector<int> ah_ptr, ah_loc; // arrowhead of each supernode (as for the Newton system)
     std::vector<int> br_pos;         // 4 per branch: A-array index (ff, ft, tf, tt) or -1
     std::vector<double> br_val;      // 4 per branch: B contributions (ff, ft, tf, tt)
+    std::vector<int> diag_pos;       // per bus: A-array index of its diagonal or -1
   };
   FDSystem bp[2], bpp[2];            // [0] = XB, [1] = BX
   std::vector<int> bpp_order;

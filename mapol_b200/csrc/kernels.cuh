@@ -39,6 +39,7 @@ __device__ __forceinline__ size_t at32(int g, long long n, long long e, int lane
 struct DevGrid {
   int nb, nfree, ngroups, n_jac, nA_jac;
   int angle_mode;
+  int nslot, noltc;         // per-case control slots / controlled taps (0: none)
   const int* y_rowptr;
   const int* y_col;
   const double2* y_val;
@@ -62,6 +63,12 @@ struct DevGrid {
   int* group_active;        // [ngroups]
   int* any_active;          // [1]
   int* it_ptr;              // [1] Newton iterations done (graph replays read it)
+  // per-case controls (null when none are set)
+  const int* y_slot;        // [nnzY] control slot of a Ybus position or -1
+  const double2* ctl_dy;    // [g][nslot][32] change of the Ybus entry at each slot
+  const int* br_ctl;        // [nbr] index among the controlled taps or -1
+  const double2* ctl_bry;   // [g][4 noltc][32] admittances (ff, ft, tf, tt) of the controlled taps
+  const double2* ctl_bdy;   // [g][4 noltc][32] their dY/dg (adjoint)
 };
 
 struct DevLU {
@@ -135,6 +142,44 @@ __device__ __forceinline__ double2 ycase(const DevGrid& d, const LaneOut& o, int
     if (p == q.w) { const double2 t = by[3]; y.x -= t.x; y.y -= t.y; }
   }
   return y;
+}
+
+// Ybus entry p of this case: ycase() on rows an outage touches, plus the change a
+// per-case control (tap or shunt susceptance) makes at p.
+// CTL = false compiles the correction out (kernels whose register budget is tight
+// have a variant per case; the others pass true and test d.y_slot).
+template <bool CTL = true>
+__device__ __forceinline__ double2 yentry(const DevGrid& d, const LaneOut& o, bool touched, int p, int g, int lane) {
+  double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
+  if (CTL && d.y_slot) {
+    const int s = d.y_slot[p];
+    if (s >= 0) {
+      const double2 t = d.ctl_dy[at32(g, d.nslot, s, lane)];
+      y.x += t.x;
+      y.y += t.y;
+    }
+  }
+  return y;
+}
+
+// Branch k's four admittances (ff, ft, tf, tt) in this case: the base values, or the
+// case's own when its tap is a per-case control.
+__device__ __forceinline__ void branch_y(const DevGrid& d, int k, int g, int lane, double2 y[4]) {
+  const int j = d.br_ctl ? d.br_ctl[k] : -1;
+  if (j < 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) y[q] = d.br_y[4 * k + q];
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) y[q] = d.ctl_bry[at32(g, 4 * d.noltc, 4 * j + q, lane)];
+  }
+}
+
+__device__ __forceinline__ bool outaged(const LaneOut& o, int k) {
+  bool out = false;
+#pragma unroll
+  for (int q = 0; q < kMaxOut; ++q) out |= (o.e[q] == k);
+  return out;
 }
 
 __device__ __forceinline__ double vangle(double2 v, int mode) {
@@ -215,7 +260,7 @@ constexpr int kRowsPerBlock = 64;
 //   V_i = a + jb, V_j = c + jd, yv = Y_ij V_j, w = yv / |V_j|, I = Ibus_i if i == j else 0
 //   dP/dVa = -b (I_r - yv_r) - a (-I_i + yv_i)     dP/dVm = a w_r + b w_i + (I_r c + I_i d)/|V_j|
 //   dQ/dVa = -b (-I_i + yv_i) + a (I_r - yv_r)     dQ/dVm = -a w_i + b w_r + (I_r d - I_i c)/|V_j|
-template <typename T, bool JAC>
+template <typename T, bool JAC, bool CTL>
 __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
   const int g = blockIdx.y;
   if (!d.group_active[g]) return;
@@ -231,7 +276,7 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
     const int p0 = d.y_rowptr[i], p1 = d.y_rowptr[i + 1];
     const bool touched = row_touched(o, d.y_diag[i]);
     for (int p = p0; p < p1; ++p) {
-      const double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
+      const double2 y = yentry<CTL>(d, o, touched, p, g, lane);
       const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
       ib.x += y.x * v.x - y.y * v.y;
       ib.y += y.x * v.y + y.y * v.x;
@@ -257,7 +302,7 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
         const int4 jp = d.jpos[p];
         if (jp.x < 0 && jp.y < 0 && jp.z < 0 && jp.w < 0) continue;
         const int j = d.y_col[p];
-        const double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
+        const double2 y = yentry<CTL>(d, o, touched, p, g, lane);
         const double2 vj = d.V[at32(g, d.nb, j, lane)];
         const double cc = vj.x, dd = vj.y;
         const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
@@ -325,7 +370,7 @@ __global__ void __launch_bounds__(256) k_mismatch_fd(DevGrid d, DevFD f, T* xp, 
     double2 ib = make_double2(0.0, 0.0);
     const bool touched = row_touched(o, d.y_diag[i]);
     for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
-      const double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
+      const double2 y = yentry(d, o, touched, p, g, lane);
       const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
       ib.x += y.x * v.x - y.y * v.y;
       ib.y += y.x * v.y + y.y * v.x;
@@ -648,7 +693,7 @@ __global__ void __launch_bounds__(256) k_mismatch_eval(DevGrid d, const double2*
     double2 ib = make_double2(0.0, 0.0);
     const bool touched = row_touched(o, d.y_diag[i]);
     for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
-      const double2 y = touched ? ycase(d, o, p, d.y_val[p]) : d.y_val[p];
+      const double2 y = yentry(d, o, touched, p, c >> 5, c & 31);
       const double2 vj = vc[d.y_col[p]];
       ib.x += y.x * vj.x - y.y * vj.y;
       ib.y += y.x * vj.y + y.y * vj.x;
@@ -696,13 +741,11 @@ __global__ void __launch_bounds__(256) k_branch_flow(DevGrid d, int nbr, int nca
   const int k0 = blockIdx.x * 64;
   const int k1 = min(nbr, k0 + 64);
   for (int k = k0 + warp; k < k1; k += 8) {
-    bool out = false;
-#pragma unroll
-    for (int q = 0; q < kMaxOut; ++q) out |= (o.e[q] == k);
     double2 sf = make_double2(0.0, 0.0), stt = make_double2(0.0, 0.0);
-    if (!out) {
+    if (!outaged(o, k)) {
       const int2 ft = d.br_ft[k];
-      const double2* y = d.br_y + 4 * k;
+      double2 y[4];
+      branch_y(d, k, g, lane, y);
       const double2 vf = d.V[at32(g, d.nb, ft.x, lane)], vt = d.V[at32(g, d.nb, ft.y, lane)];
       const double2 i_f = make_double2(y[0].x * vf.x - y[0].y * vf.y + y[1].x * vt.x - y[1].y * vt.y,
                                        y[0].x * vf.y + y[0].y * vf.x + y[1].x * vt.y + y[1].y * vt.x);
@@ -757,12 +800,10 @@ __global__ void __launch_bounds__(256) k_adj_dldx(DevGrid d, int nbr, const doub
   load_outages(d, c, o);
   const int k1 = min(nbr, (int)(blockIdx.x + 1) * 64);
   for (int k = blockIdx.x * 64 + warp; k < k1; k += 8) {
-    bool out = false;
-#pragma unroll
-    for (int q = 0; q < kMaxOut; ++q) out |= (o.e[q] == k);
-    if (out) continue;
+    if (outaged(o, k)) continue;
     const int2 ft = d.br_ft[k];
-    const double2* y = d.br_y + 4 * k;
+    double2 y[4];
+    branch_y(d, k, grp, lane, y);
     const double2 vf = d.V[at32(grp, d.nb, ft.x, lane)], vt = d.V[at32(grp, d.nb, ft.y, lane)];
     // W = Vf conj(Yft Vt)
     const double2 yv = make_double2(y[1].x * vt.x - y[1].y * vt.y, y[1].x * vt.y + y[1].y * vt.x);
@@ -891,14 +932,15 @@ __global__ void __launch_bounds__(256) k_adj_grad_branch(DevGrid d, int nbr, int
   const int k1 = min(nbr, (int)(blockIdx.x + 1) * 64);
   for (int k = blockIdx.x * 64 + warp; k < k1; k += 8) {
     if (c >= ncases) continue;
-    bool out = false;
-#pragma unroll
-    for (int q = 0; q < kMaxOut; ++q) out |= (o.e[q] == k);
     double rg = 0.0, rb = 0.0;
-    if (ok && !out) {
+    if (ok && !outaged(o, k)) {
       const int2 ft = d.br_ft[k];
-      const double2* y = d.br_y + 4 * k;
-      const double2* a = br_dy + 4 * k;
+      double2 y[4], a[4];
+      branch_y(d, k, grp, lane, y);
+      const int jc = d.br_ctl ? d.br_ctl[k] : -1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        a[q] = jc < 0 ? br_dy[4 * k + q] : d.ctl_bdy[at32(grp, 4 * d.noltc, 4 * jc + q, lane)];
       const double2 vf = d.V[at32(grp, d.nb, ft.x, lane)], vt = d.V[at32(grp, d.nb, ft.y, lane)];
       // Df = Vf conj(a_ff Vf + a_ft Vt), Dt = Vt conj(a_tf Vf + a_tt Vt)
       const double2 u = make_double2(a[0].x * vf.x - a[0].y * vf.y + a[1].x * vt.x - a[1].y * vt.y,
@@ -928,6 +970,139 @@ __global__ void __launch_bounds__(256) k_adj_grad_branch(DevGrid d, int nbr, int
     }
     if (gg) gg[(size_t)c * nbr + k] = rg;
     if (gb) gb[(size_t)c * nbr + k] = rb;
+  }
+}
+
+// ---------------------------------------------------------------- per-case controls
+// The optimiser's structures (pso/Particula.h:26-60): AVR = |V| set-point of a PV or
+// slack bus (runpf.h:524-541), OLTC = tap ratio of a branch and ShC = shunt
+// susceptance of a bus (makeYbus.h:313-332).  values[g][k][32] holds control k of
+// every case; a tap or shunt changes the Ybus entries at its slots, which yentry()
+// adds to the base value.
+struct DevCtl {
+  int nc, navr, noltc, nshc, nslot;
+  const double* val;        // [g][nc][32]
+  const int2* avr;          // (bus, value column)
+  const int2* oltc;         // (branch, value column)
+  const double* oltc_par;   // 8 per tap: Ys (re, im), b/2, cos, sin of the shift, Ys with r = 0 (re, im), 0
+  const int2* shc;          // (bus, value column)
+  const double* shc_base;   // base Bsh of each controlled shunt
+  const int* slot_ptr;      // [nslot + 1]
+  const int2* slot_ent;     // (q, j): q < 3 entry q (ff, ft, tf) of tap j; q == 3 shunt j
+};
+
+// Admittances and dY/dg of every controlled tap in every case (branch_admittance with
+// the case's tap; all zero for a branch out of service).  Thread per (tap, lane).
+__global__ void k_ctl_branch(DevCtl t, int ngroups, double2* __restrict__ bry, double2* __restrict__ bdy) {
+  const size_t total = (size_t)ngroups * t.noltc * 32;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < total; id += (size_t)gridDim.x * blockDim.x) {
+    const int lane = (int)(id & 31);
+    const size_t rest = id >> 5;
+    const int j = (int)(rest % t.noltc), g = (int)(rest / t.noltc);
+    const double tap = t.val[at32(g, t.nc, t.oltc[j].y, lane)];
+    const double* pr = t.oltc_par + 8 * j;
+    const double ysr = pr[0], ysi = pr[1], bc2 = pr[2];
+    const double tr = tap * pr[3], ti = tap * pr[4];
+    const double t2 = tr * tr + ti * ti;
+    const double ytr = ysr, yti = ysi + bc2;
+    const bool on = ysr != 0.0 || ysi != 0.0 || bc2 != 0.0;
+    double2 y[4], a[4];
+    y[0] = make_double2(ytr / t2, yti / t2);
+    y[1] = make_double2(-(ysr * tr - ysi * ti) / t2, -(ysr * ti + ysi * tr) / t2);
+    y[2] = make_double2(-(ysr * tr + ysi * ti) / t2, -(ysi * tr - ysr * ti) / t2);
+    y[3] = make_double2(ytr, yti);
+    a[0] = make_double2(1.0 / t2, 0.0);
+    a[1] = make_double2(-tr / t2, -ti / t2);
+    a[2] = make_double2(-tr / t2, ti / t2);
+    a[3] = make_double2(1.0, 0.0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const size_t k = at32(g, 4 * t.noltc, 4 * j + q, lane);
+      bry[k] = y[q];
+      bdy[k] = on ? a[q] : make_double2(0.0, 0.0);
+    }
+  }
+}
+
+// Per case and slot: the sum of the changes the controls make at that Ybus position
+// (a tap whose branch the case outages contributes nothing: ycase() removes the
+// branch's base admittance).  Thread per (slot, lane).
+__global__ void k_ctl_ydelta(DevGrid d, DevCtl t, const double2* __restrict__ bry, double2* __restrict__ dy) {
+  const size_t total = (size_t)d.ngroups * t.nslot * 32;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < total; id += (size_t)gridDim.x * blockDim.x) {
+    const int lane = (int)(id & 31);
+    const size_t rest = id >> 5;
+    const int s = (int)(rest % t.nslot), g = (int)(rest / t.nslot);
+    LaneOut o;
+    load_outages(d, g * 32 + lane, o);
+    double2 acc = make_double2(0.0, 0.0);
+    for (int e = t.slot_ptr[s]; e < t.slot_ptr[s + 1]; ++e) {
+      const int2 en = t.slot_ent[e];
+      if (en.x < 3) {
+        const int k = t.oltc[en.y].x;
+        if (outaged(o, k)) continue;
+        const double2 nv = bry[at32(g, 4 * t.noltc, 4 * en.y + en.x, lane)];
+        const double2 bv = d.br_y[4 * k + en.x];
+        acc.x += nv.x - bv.x;
+        acc.y += nv.y - bv.y;
+      } else {
+        acc.y += t.val[at32(g, t.nc, t.shc[en.y].y, lane)] - t.shc_base[en.y];
+      }
+    }
+    dy[at32(g, t.nslot, s, lane)] = acc;
+  }
+}
+
+// AVR set-points: V_i = value e^{j Va_i} (runpf.h:524-541).  Thread per (AVR, lane),
+// after k_init.
+__global__ void k_ctl_vm(DevGrid d, DevCtl t) {
+  const size_t total = (size_t)d.ngroups * t.navr * 32;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < total; id += (size_t)gridDim.x * blockDim.x) {
+    const int lane = (int)(id & 31);
+    const size_t rest = id >> 5;
+    const int j = (int)(rest % t.navr), g = (int)(rest / t.navr);
+    const int2 a = t.avr[j];
+    const double2 v0 = d.v0[a.x];
+    double sn, cs;
+    sincos(atan2(v0.y, v0.x), &sn, &cs);
+    const double vm = t.val[at32(g, t.nc, a.y, lane)];
+    d.V[at32(g, d.nb, a.x, lane)] = make_double2(vm * cs, vm * sn);
+  }
+}
+
+// B'' of every case with its controls (B' has taps and shunts zeroed, makeB.h:311-324,
+// so it has none): at each slot inside B'' (pos >= 0), the change of -Im(Y'') that the
+// case's taps (phase shift 0; r = 0 in BX) and shunts make.  Thread per (slot, lane).
+template <typename T>
+__global__ void k_fd_ctl(DevGrid d, DevCtl t, int variant, int nA, const int* __restrict__ slot_pos,
+                         const double4* __restrict__ br_bval, T* __restrict__ A) {
+  const size_t total = (size_t)d.ngroups * t.nslot * 32;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < total; id += (size_t)gridDim.x * blockDim.x) {
+    const int lane = (int)(id & 31);
+    const size_t rest = id >> 5;
+    const int s = (int)(rest % t.nslot), g = (int)(rest / t.nslot);
+    const int pos = slot_pos[s];
+    if (pos < 0) continue;
+    LaneOut o;
+    load_outages(d, g * 32 + lane, o);
+    double acc = 0.0;
+    for (int e = t.slot_ptr[s]; e < t.slot_ptr[s + 1]; ++e) {
+      const int2 en = t.slot_ent[e];
+      if (en.x < 3) {
+        const int k = t.oltc[en.y].x;
+        if (outaged(o, k)) continue;
+        const double* pr = t.oltc_par + 8 * en.y;
+        const double ysi = variant == 1 ? pr[6] : pr[1];
+        const double tap = t.val[at32(g, t.nc, t.oltc[en.y].y, lane)];
+        const double nv = en.x == 0 ? -(ysi + pr[2]) / (tap * tap) : ysi / tap;
+        const double4 bv = br_bval[k];
+        acc += nv - (en.x == 0 ? bv.x : en.x == 1 ? bv.y : bv.z);
+      } else {
+        acc -= t.val[at32(g, t.nc, t.shc[en.y].y, lane)] - t.shc_base[en.y];
+      }
+    }
+    const size_t idx = at32(g, nA, pos, lane);
+    A[idx] = (T)((double)A[idx] + acc);
   }
 }
 

@@ -365,11 +365,13 @@ static void build_fd(GridSymbolic& g, const mpf_bus* buses, const mpf_branch* br
   for (int e = 0; e < g.nbr; ++e)
     for (int q : {2, 3})
       if (fd.br_pos[4 * e + q] >= 0) fd.base[fd.br_pos[4 * e + q]] += fd.br_val[4 * e + q];
+  fd.diag_pos.assign(g.nb, -1);
   for (int i = 0; i < g.nb; ++i) {
     if (var_of_bus[i] < 0) continue;
     // B' has Bsh zeroed (makeB.h:320-323); B'' keeps the bus shunt: -Im(j Bsh)
     const double sh = is_bp ? 0.0 : -buses[i].bsh;
-    fd.base[a_index[y_to_entry[g.y_diag[i]]]] += sh;
+    fd.diag_pos[i] = a_index[y_to_entry[g.y_diag[i]]];
+    fd.base[fd.diag_pos[i]] += sh;
   }
 }
 

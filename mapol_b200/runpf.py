@@ -45,13 +45,13 @@ class PowerFlow:
     """One grid on one GPU (mpf_create).  Replaces hybrid_init / hybrid_free."""
 
     def __init__(self, buses, branches, max_it_nr=MAX_IT_NR, max_it_fd=MAX_IT_FD, tol=EPS,
-                 angle_mode=0, device=0):
+                 angle_mode=0, device=0, use_graph=1):
         self.buses = np.ascontiguousarray(buses, dtype=T.BUS_DTYPE)
         self.branches = np.ascontiguousarray(branches, dtype=T.BRANCH_DTYPE)
         opt = T.Options()
         lib().mpf_default_options(ctypes.byref(opt))
         opt.max_it_nr, opt.max_it_fd, opt.tol = max_it_nr, max_it_fd, tol
-        opt.angle_mode, opt.device = angle_mode, device
+        opt.angle_mode, opt.device, opt.use_graph = angle_mode, device, use_graph
         h = ctypes.c_void_p()
         rc = lib().mpf_create(ptr(self.buses), len(self.buses), ptr(self.branches), len(self.branches),
                               ctypes.byref(opt), ctypes.byref(h))
@@ -94,6 +94,20 @@ class PowerFlow:
         sb = None if sbus is None else np.ascontiguousarray(sbus, dtype=np.float64)
         self._check(lib().mpf_set_cases(self._h, len(cases), ptr(offs), ptr(flat), ptr(sb)))
         self.n_cases = len(cases)
+
+    def set_controls(self, controls, values):
+        """Per-case control overrides of the current cases (mpf_set_controls).
+        controls: sequence of (kind, index) with kind CTRL_AVR (PV/slack bus |V|
+        set-point), CTRL_OLTC (tap ratio of a tapped branch) or CTRL_SHC (bus shunt
+        susceptance); values: (n_cases, n_controls).  An empty sequence clears."""
+        ctl = np.array([tuple(c) for c in controls], dtype=T.CONTROL_DTYPE)
+        if len(ctl) == 0:
+            self._check(lib().mpf_set_controls(self._h, 0, None, None))
+            return
+        val = np.ascontiguousarray(values, dtype=np.float64)
+        if val.shape != (self.n_cases, len(ctl)):
+            raise ValueError(f"values must be ({self.n_cases}, {len(ctl)}), got {val.shape}")
+        self._check(lib().mpf_set_controls(self._h, len(ctl), ptr(ctl), ptr(val)))
 
     def solve(self, alg=NR, precision=FP64, stream=None):
         self._check(lib().mpf_solve(self._h, alg, precision, stream))
