@@ -477,10 +477,17 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
     T* __restrict__ x, int* __restrict__ status, const int* __restrict__ group_active, int with_rhs) {
   constexpr int SLOTS = TEAM / G;
   constexpr int LPG = 32 / G;  // lane chunks per group
+  // slots of a lane form RSL row slots x CG column groups: rows are dealt to the
+  // row slots, and each column group takes a contiguous share of a row's columns
+  // (fronts have fewer rows than a 256-thread team has slots when G is small)
+  constexpr int RSL = SLOTS < 32 ? SLOTS : 32;
+  constexpr int CG = SLOTS / RSL;
+  constexpr int U = 8;  // loads issued before the dependent shared-memory stores
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int teams = blockDim.x / TEAM;
   const int team = threadIdx.x / TEAM, tid = threadIdx.x % TEAM;
   const int slot = tid / G, l = tid % G;
+  const int rs = slot % RSL, cg = slot / RSL;
   T* F = reinterpret_cast<T*>(smem_raw) + (size_t)team * fcap * front_stride(fcap) * G;
   const long long nchunks = (long long)ngroups * LPG;
   const long long ntasks = (long long)nsn_l * nchunks;
@@ -506,14 +513,36 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
       const int m = L.sn_f[ch2] - L.sn_w[ch2];
       const int* rel = L.relmap + L.rel_ptr[ch2];
       const long long cbo = L.cb_off[ch2];
-      for (int a = slot; a < m; a += SLOTS) {
-        const int ra = rel[a];
+      // column share of this column group
+      const int b0 = (m * cg) / CG, b1 = (m * (cg + 1)) / CG;
+      for (int a = rs; a < m; a += RSL) {
+        T* dst = &FR(rel[a], 0);
         const T* src = cb + at32(g, L.sumcb, cbo + (long long)a * m, lane);
-        for (int b = 0; b < m; ++b) FR(ra, rel[b]) += src[(size_t)b * 32];
-        if (with_rhs) FR(ra, f) += cbr[at32(g, L.sumcbr, L.cbr_off[ch2] + a, lane)];
+        int b = b0;
+        for (; b + U <= b1; b += U) {
+          int rb[U];
+          T v[U], o[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            rb[u] = rel[b + u] * G;
+            v[u] = src[(size_t)(b + u) * 32];
+          }
+          // rel is injective: the U destinations are distinct
+#pragma unroll
+          for (int u = 0; u < U; ++u) o[u] = dst[rb[u]];
+#pragma unroll
+          for (int u = 0; u < U; ++u) dst[rb[u]] = o[u] + v[u];
+        }
+        for (; b < b1; ++b) dst[rel[b] * G] += src[(size_t)b * 32];
+        if (with_rhs && cg == 0) FR(rel[a], f) += cbr[at32(g, L.sumcbr, L.cbr_off[ch2] + a, lane)];
       }
       team_sync<TEAM>();
     }
+    // Right-looking partial LU of the w pivots, one team barrier per pivot.  At
+    // pivot p every thread reads the unscaled column p (l_ip = F(i,p) / F(p,p));
+    // the scaled values are written back one pivot later, when no thread reads
+    // column p any more (and after the loop for the last pivot).
+    T inv_prev = (T)0;
     for (int p = 0; p < w; ++p) {
       T piv = FR(p, p);
       if (!(fabs((double)piv) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)piv) <= DBL_MAX)) {
@@ -521,34 +550,61 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
         piv = (T)1;
       }
       const T inv = (T)1 / piv;
-      // each slot owns rows i = p+1+slot, p+1+slot+SLOTS, ...: scale L(i,p), then
-      // update row i with the (broadcast) pivot row
-      for (int i = p + 1 + slot; i < f; i += SLOTS) {
-        const T lip = FR(i, p) * inv;
-        FR(i, p) = lip;
-        for (int q = p + 1; q < ncols; ++q) FR(i, q) -= lip * FR(p, q);
+      if (p > 0 && cg == CG - 1)
+        for (int i = p + rs; i < f; i += RSL) FR(i, p - 1) *= inv_prev;
+      const int nq = ncols - (p + 1);
+      const int q0 = p + 1 + (nq * cg) / CG, q1 = p + 1 + (nq * (cg + 1)) / CG;
+      const T* rp = &FR(p, 0);
+      for (int i = p + 1 + rs; i < f; i += RSL) {
+        T* ri = &FR(i, 0);
+        const T lip = ri[p * G] * inv;
+        int q = q0;
+        for (; q + U <= q1; q += U) {
+          T a[U], b[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            a[u] = rp[(q + u) * G];
+            b[u] = ri[(q + u) * G];
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) ri[(q + u) * G] = b[u] - lip * a[u];
+        }
+        for (; q < q1; ++q) ri[q * G] -= lip * rp[q * G];
       }
+      inv_prev = inv;
+      team_sync<TEAM>();
+    }
+    if (w > 0) {
+      if (cg == CG - 1)
+        for (int i = w + rs; i < f; i += RSL) FR(i, w - 1) *= inv_prev;
       team_sync<TEAM>();
     }
     const long long po = L.pan_off[s];
     // U-panel: rows 0..w-1, all f columns; L-panel: rows w..f-1, columns 0..w-1
-    for (int p = slot; p < w; p += SLOTS) {
-      T* dst = pan + at32(g, L.nnz, po + (long long)p * f, lane);
-      for (int q = 0; q < f; ++q) dst[(size_t)q * 32] = FR(p, q);
+    {
+      const int c0 = (f * cg) / CG, c1 = (f * (cg + 1)) / CG;
+      for (int p = rs; p < w; p += RSL) {
+        T* dst = pan + at32(g, L.nnz, po + (long long)p * f, lane);
+        for (int q = c0; q < c1; ++q) dst[(size_t)q * 32] = FR(p, q);
+      }
     }
     const int m = f - w;
-    for (int i = slot; i < m; i += SLOTS) {
-      T* dst = pan + at32(g, L.nnz, po + (long long)w * f + (long long)i * w, lane);
-      for (int q = 0; q < w; ++q) dst[(size_t)q * 32] = FR(w + i, q);
+    {
+      const int c0 = (w * cg) / CG, c1 = (w * (cg + 1)) / CG;
+      for (int i = rs; i < m; i += RSL) {
+        T* dst = pan + at32(g, L.nnz, po + (long long)w * f + (long long)i * w, lane);
+        for (int q = c0; q < c1; ++q) dst[(size_t)q * 32] = FR(w + i, q);
+      }
     }
     if (with_rhs)
       for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, rows[p], lane)] = FR(p, f);
     if (L.sn_parent[s] >= 0) {
       const long long cbo = L.cb_off[s];
-      for (int a = slot; a < m; a += SLOTS) {
+      const int c0 = (m * cg) / CG, c1 = (m * (cg + 1)) / CG;
+      for (int a = rs; a < m; a += RSL) {
         T* dst = cb + at32(g, L.sumcb, cbo + (long long)a * m, lane);
-        for (int b = 0; b < m; ++b) dst[(size_t)b * 32] = FR(w + a, w + b);
-        if (with_rhs) cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = FR(w + a, f);
+        for (int b = c0; b < c1; ++b) dst[(size_t)b * 32] = FR(w + a, w + b);
+        if (with_rhs && cg == 0) cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = FR(w + a, f);
       }
     }
 #undef FR
