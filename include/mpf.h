@@ -111,7 +111,10 @@ typedef struct mpf_options {
                           src/util/complexUtils.h:21-23 (loses the quadrant) */
   int32_t device;      /* CUDA device ordinal, default 0 */
   int32_t use_graph;   /* 1: capture the Newton iteration in a CUDA graph (default 1) */
-  int32_t reserved[5];
+  int32_t autotune;    /* 1: time the candidate kernels of every factorisation launch on
+                          the first solve of a batch size and keep the fastest (default 1);
+                          0: fixed heuristic */
+  int32_t reserved[4];
 } mpf_options;
 
 /* Per-kernel device time of the last mpf_solve (CUDA events on the solve stream),

@@ -83,7 +83,8 @@ class Options(ctypes.Structure):
         ("angle_mode", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 5),
+        ("autotune", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 

@@ -10,7 +10,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <set>
@@ -88,11 +90,20 @@ struct Launch {
   int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
 };
 
+// Kernel of one factorisation launch: kind 0 = warp teams (k_mf_factor<T, ge, 32>,
+// tpb teams per block), 1 = 256-thread teams with the LU in shared memory, 2 = the
+// same with the LU in registers (TT x TT tile per thread)
+struct FactorChoice {
+  int kind, ge, tt, tpb;
+};
+
 struct LUSystem {
   LUSymbolic sym;
   DevBuf sn_w, sn_f, sn_rptr, sn_rows, child_ptr, child_list, sn_parent, rel_ptr, relmap, ah_ptr, ah_loc;
   DevBuf pan_off, cb_off, cbr_off, lev_sn;
   std::vector<Launch> factor_sched;  // ascending levels
+  // autotuned kernel of every factor_sched launch, per (precision, case groups)
+  std::map<std::pair<int, int>, std::vector<FactorChoice>> tuned;
   std::vector<Launch> level_sched;   // one launch per level (solves), ascending
   int nA = 0;
   // values per precision [0] = FP64, [1] = FP32
@@ -209,6 +220,17 @@ struct Prec<float> { static constexpr int idx = 1; static constexpr int G = 8; }
 
 // Opt every kernel that may take more than 48 KB of dynamic shared memory into the
 // full 227 KB, once per device and value type, before any launch or graph capture.
+template <typename T, int G>
+void set_reg_attrs(int smax) {
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, G, 256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, G, 256, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, G, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  if constexpr (G * sizeof(T) <= 8) {
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, G, 256, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+    CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, G, 256, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  }
+}
+
 template <typename T>
 void ensure_attrs(int device) {
   static std::mutex mu;
@@ -223,6 +245,9 @@ void ensure_attrs(int device) {
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 1, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  set_reg_attrs<T, 1>(smax);
+  set_reg_attrs<T, 2>(smax);
+  if constexpr (sizeof(T) == 4) set_reg_attrs<T, 4>(smax);
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
@@ -232,15 +257,23 @@ void ensure_attrs(int device) {
   done[device] = true;
 }
 
-template <typename T, int G, int TEAM>
+// dynamic shared memory of a factor launch: the fronts, plus the pivot column/row
+// buffers of the register LU
+template <typename T, int G, int TT>
+size_t factor_smem(int fcap, int teams_per_block) {
+  size_t b = (size_t)fcap * front_stride(fcap) * G * sizeof(T) * teams_per_block;
+  if (TT > 0) b += (size_t)(2 * fcap + 2 * (fcap + 1)) * G * sizeof(T);
+  return b;
+}
+
+template <typename T, int G, int TEAM, int TT = 0>
 void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x,
                        int* status, const int* group_active, int with_rhs, cudaStream_t st, int teams_per_block) {
-  const size_t team_elems = (size_t)ln.fcap * front_stride(ln.fcap) * G;
-  const size_t smem = team_elems * sizeof(T) * teams_per_block;
+  const size_t smem = factor_smem<T, G, TT>(ln.fcap, teams_per_block);
   const long long ntasks = (long long)ln.count * ngroups * (32 / G);
   long long blocks = (ntasks + teams_per_block - 1) / teams_per_block;
   blocks = std::min<long long>(blocks, 148LL * 32);
-  k_mf_factor<T, G, TEAM><<<(unsigned)blocks, TEAM * teams_per_block, smem, st>>>(
+  k_mf_factor<T, G, TEAM, TT><<<(unsigned)blocks, TEAM * teams_per_block, smem, st>>>(
       sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups, ln.fcap, A, pan, cb, cbr, x, status,
       group_active, with_rhs);
   CUDA_TRY(cudaGetLastError());
@@ -263,37 +296,200 @@ void launch_factor_ge(int ge, const LUSystem& sys, const Launch& ln, int ngroups
   }
 }
 
+// Register-LU tiles: TT x TT entries per thread covers fronts with f + 1 <= 16 TT
+// (right-hand side column included).  Lane chunks: up to 16 bytes (one thread
+// per entry); 4 FP32 lanes only up to TT = 4, 2 FP64 lanes up to TT = 4, to keep
+// the tile within about 128 registers.
+constexpr int kRegTTMax = 6;
+inline int reg_tt(int fcap) { return std::max(2, (fcap + 1 + 15) / 16); }
+template <typename T>
+int reg_lanes_max(int tt) {
+  if (sizeof(T) == 4) return tt <= 4 ? 4 : 2;
+  return tt <= 4 ? 2 : 1;
+}
+
+template <typename T, int G>
+void launch_factor_reg_g(int tt, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb,
+                         T* cbr, T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
+  switch (tt) {
+    case 2: launch_factor_one<T, G, 256, 2>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
+    case 3: launch_factor_one<T, G, 256, 3>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
+    case 4: launch_factor_one<T, G, 256, 4>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
+    case 5:
+    case 6:
+      if constexpr (G * sizeof(T) <= 8) {
+        if (tt == 5) launch_factor_one<T, G, 256, 5>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+        else launch_factor_one<T, G, 256, 6>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+        break;
+      }
+      [[fallthrough]];
+    default:
+      throw MpfError{MPF_ERR_INTERNAL, "no register-LU kernel for this tile and lane count"};
+  }
+}
+
+template <typename T>
+void launch_factor_reg(int ge, int tt, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb,
+                       T* cbr, T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
+  if (ge >= 4) {
+    if constexpr (sizeof(T) == 4)
+      launch_factor_reg_g<T, 4>(tt, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+    else
+      throw MpfError{MPF_ERR_INTERNAL, "no register-LU kernel for this lane count"};
+  } else if (ge == 2) {
+    launch_factor_reg_g<T, 2>(tt, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+  } else {
+    launch_factor_reg_g<T, 1>(tt, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+  }
+}
+
+inline size_t factor_smem_rt(int fcap, int ge, int teams, int tt, size_t wsize) {
+  size_t b = (size_t)fcap * front_stride(fcap) * ge * wsize * teams;
+  if (tt > 0) b += (size_t)(4 * fcap + 2) * ge * wsize;
+  return b;
+}
+
+// The fixed rule (used without autotuning, and as the first candidate): thread per
+// case for fronts up to 8, warp teams up to 24, 256-thread teams above (register
+// LU up to 16 kRegTTMax - 1 rows); lane chunks shrink while a level has too few
+// tasks to fill the GPU or the front would not fit in shared memory.
+template <typename T>
+FactorChoice heuristic_choice(const Launch& ln, int ngroups) {
+  constexpr int G = Prec<T>::G;
+  const long long lanes_tasks = (long long)ln.count * ngroups;
+  if (ln.cls == CLS_S && lanes_tasks < kMinWarpTasks) return {1, 32, 0, 1};
+  if ((ln.cls == CLS_M1 || ln.cls == CLS_M) && lanes_tasks * (32 / G) < kMinWarpTasks) {
+    int ge = G;
+    while (ge > 1 && lanes_tasks * (32 / ge) < kMinBlockTasks) ge /= 2;
+    return {1, ge, 0, 1};
+  }
+  if (ln.cls == CLS_S) return {0, 32, 0, sizeof(T) == 8 ? 4 : 8};
+  if (ln.cls == CLS_M1) return {0, G, 0, 8};
+  if (ln.cls == CLS_M) return {0, G, 0, 4};
+  const size_t per_lane = (size_t)ln.fcap * front_stride(ln.fcap) * sizeof(T);
+  int ge = G;
+  while (ge > 1 && (per_lane * ge > kSmemMax || lanes_tasks * (32 / ge) < kMinBlockTasks)) ge /= 2;
+  return {1, ge, 0, 1};
+}
+
+// Every kernel that can run the launch: warp teams (2 to 8 teams per block), the
+// 256-thread shared-memory LU at each lane chunk, and the register LU at each
+// lane chunk its tile allows, as long as the fronts fit in shared memory.
+template <typename T>
+std::vector<FactorChoice> factor_candidates(const Launch& ln, int ngroups) {
+  constexpr int G = Prec<T>::G;
+  const size_t ws = sizeof(T);
+  std::vector<FactorChoice> c{heuristic_choice<T>(ln, ngroups)};
+  auto add = [&](FactorChoice x) {
+    for (const auto& y : c)
+      if (y.kind == x.kind && y.ge == x.ge && y.tt == x.tt && y.tpb == x.tpb) return;
+    c.push_back(x);
+  };
+  if (ln.fcap <= kFmaxS) {
+    for (int tpb : {8, 4})
+      if (factor_smem_rt(ln.fcap, 32, tpb, 0, ws) <= kSmemMax) add({0, 32, 0, tpb});
+    add({1, 32, 0, 1});
+  }
+  for (int tpb : {8, 4, 2})
+    if (factor_smem_rt(ln.fcap, G, tpb, 0, ws) <= kSmemMax) add({0, G, 0, tpb});
+  for (int ge = G; ge >= 1; ge /= 2)
+    if (factor_smem_rt(ln.fcap, ge, 1, 0, ws) <= kSmemMax) add({1, ge, 0, 1});
+  const int tt = reg_tt(ln.fcap);
+  if (ln.fcap > kFmaxS && tt <= kRegTTMax)
+    for (int ge = reg_lanes_max<T>(tt); ge >= 1; ge /= 2)
+      if (factor_smem_rt(ln.fcap, ge, 1, tt, ws) <= kSmemMax) add({2, ge, tt, 1});
+  return c;
+}
+
+template <typename T>
+void launch_choice(const FactorChoice& ch, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan,
+                   T* cb, T* cbr, T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
+  constexpr int G = Prec<T>::G;
+  if (ch.kind == 0) {
+    if (ch.ge == 32)
+      launch_factor_one<T, 32, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, ch.tpb);
+    else
+      launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, ch.tpb);
+  } else if (ch.kind == 1) {
+    if (ch.ge == 32)
+      launch_factor_one<T, 32, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+    else
+      launch_factor_ge<T>(ch.ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+  } else {
+    launch_factor_reg<T>(ch.ge, ch.tt, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+  }
+}
+
 template <typename T>
 void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x, int* status,
                    const int* group_active, int with_rhs, cudaStream_t st, int* nlaunch) {
-  constexpr int G = Prec<T>::G;
-  for (const Launch& ln : sys.factor_sched) {
-    const long long lanes_tasks = (long long)ln.count * ngroups;
-    if (ln.cls == CLS_S && lanes_tasks < kMinWarpTasks) {
-      launch_factor_one<T, 32, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
-    } else if ((ln.cls == CLS_M1 || ln.cls == CLS_M) && lanes_tasks * (32 / G) < kMinWarpTasks) {
-      int ge = G;
-      while (ge > 1 && lanes_tasks * (32 / ge) < kMinBlockTasks) ge /= 2;
-      launch_factor_ge<T>(ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
-    } else if (ln.cls == CLS_S) {
-      // one case per thread, fronts up to 8 x 9
-      const int tpb = sizeof(T) == 8 ? 4 : 8;
-      launch_factor_one<T, 32, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, tpb);
-    } else if (ln.cls == CLS_M1) {
-      launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 8);
-    } else if (ln.cls == CLS_M) {
-      launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 4);
-    } else {
-      // large fronts: 256-thread team per chunk of Ge lanes; Ge shrinks (more,
-      // smaller tasks) when the level has too few tasks to fill the GPU or when a
-      // 32-byte chunk of the front would not fit in shared memory
-      const size_t per_lane = (size_t)ln.fcap * front_stride(ln.fcap) * sizeof(T);
-      int ge = G;
-      while (ge > 1 && (per_lane * ge > kSmemMax || lanes_tasks * (32 / ge) < kMinBlockTasks)) ge /= 2;
-      launch_factor_ge<T>(ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
-    }
+  const auto it = sys.tuned.find({Prec<T>::idx, ngroups});
+  const std::vector<FactorChoice>* tuned = it != sys.tuned.end() ? &it->second : nullptr;
+  for (size_t k = 0; k < sys.factor_sched.size(); ++k) {
+    const Launch& ln = sys.factor_sched[k];
+    const FactorChoice ch = tuned ? (*tuned)[k] : heuristic_choice<T>(ln, ngroups);
+    launch_choice<T>(ch, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
     ++*nlaunch;
   }
+}
+
+// Autotuner: for each launch, level by level, run every candidate twice (the
+// first run loads the kernel) and keep the one with the shortest second run
+// (CUDA events).  Runs without the right-hand side, so x is not touched; every
+// candidate computes the same panels and contribution blocks, which the next
+// level reads.  Called outside stream capture, once per (precision, groups).
+template <typename T>
+void tune_factor(LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x, int* status,
+                 const int* group_active, cudaStream_t st) {
+  if (sys.tuned.count({Prec<T>::idx, ngroups})) return;
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  std::vector<FactorChoice> best;
+  const bool log = std::getenv("MPF_TUNE_LOG") != nullptr;
+  double sum_best = 0.0, sum_heur = 0.0;
+  try {
+    for (const Launch& ln : sys.factor_sched) {
+      const std::vector<FactorChoice> cands = factor_candidates<T>(ln, ngroups);
+      FactorChoice bc = cands[0];
+      float bt = 0.0f, ht = 0.0f;
+      for (size_t i = 0; i < cands.size(); ++i) {
+        launch_choice<T>(cands[i], sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, 0, st);
+        CUDA_TRY(cudaEventRecord(e0, st));
+        launch_choice<T>(cands[i], sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, 0, st);
+        CUDA_TRY(cudaEventRecord(e1, st));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (i == 0) ht = ms;
+        if (log && std::getenv("MPF_TUNE_LOG")[0] == '2')
+          std::fprintf(stderr, "mpf tune:   cand kind %d lanes %d tile %d teams %d: %.1f us\n", cands[i].kind,
+                       cands[i].ge, cands[i].tt, cands[i].tpb, ms * 1e3);
+        if (i == 0 || ms < bt) {
+          bt = ms;
+          bc = cands[i];
+        }
+      }
+      best.push_back(bc);
+      sum_best += bt;
+      sum_heur += ht;
+      if (log)
+        std::fprintf(stderr, "mpf tune: n %d fp%d groups %d launch sn %d cls %d fcap %d: %zu candidates, "
+                     "heuristic %.1f us, best %.1f us (kind %d lanes %d tile %d teams %d)\n",
+                     sys.sym.n, (int)sizeof(T) * 8, ngroups, ln.count, ln.cls, ln.fcap, cands.size(), ht * 1e3,
+                     bt * 1e3, bc.kind, bc.ge, bc.tt, bc.tpb);
+    }
+    if (log)
+      std::fprintf(stderr, "mpf tune: n %d fp%d groups %d total heuristic %.3f ms, tuned %.3f ms\n", sys.sym.n,
+                   (int)sizeof(T) * 8, ngroups, sum_heur, sum_best);
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  sys.tuned[{Prec<T>::idx, ngroups}] = best;
 }
 
 template <typename T>
@@ -683,6 +879,10 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
   tm.end(ev);
   static const int kFam[4] = {FAM_FACT, FAM_SOLVE, FAM_UPD, FAM_MIS};
   int it = 0;
+  // pick the factorisation kernels of this batch size (first solve only), before
+  // the iteration is captured
+  if (h->opt.autotune && max_it > 0 && any_active(h, st))
+    tune_factor<T>(J, h->ngroups, A, pan, cb, cbr, x, d.status, d.group_active, st);
   auto& gph = h->nr_graph[P];
   if (h->opt.use_graph) {
     // the captured kernels hold every device pointer of d by value: capture again
@@ -770,6 +970,12 @@ void solve_fd(mpf_handle* h, cudaStream_t st, int variant) {
     }
   }
   tm.end(ev);
+  if (h->opt.autotune)
+    for (int k = 0; k < 2; ++k) {
+      LUSystem& S = *systems[k];
+      tune_factor<T>(S, h->ngroups, S.A[P].as<T>(), S.pan[P].as<T>(), S.cb[P].as<T>(), S.cbr[P].as<T>(),
+                     S.x[P].as<T>(), d.status, d.group_active, st);
+    }
   ev = tm.begin(FAM_FACT);
   for (int k = 0; k < 2; ++k) {
     LUSystem& S = *systems[k];
@@ -930,6 +1136,7 @@ void mpf_default_options(mpf_options* opt) {
   opt->angle_mode = 0;
   opt->device = 0;
   opt->use_graph = 1;
+  opt->autotune = 1;
 }
 
 const char* mpf_status_string(int32_t status) {

@@ -470,25 +470,153 @@ __device__ __forceinline__ void team_sync() {
 // rounded up to odd so that slots working on consecutive rows hit distinct banks.
 __host__ __device__ __forceinline__ int front_stride(int f) { return (f + 1) | 1; }
 
-template <typename T, int G, int TEAM>
-__global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
+// V adjacent lanes of one entry, moved as one 16-byte (or narrower) access
+template <typename T, int V>
+struct alignas(sizeof(T) * V) Lanes {
+  T v[V];
+};
+template <typename T, int V>
+__device__ __forceinline__ Lanes<T, V> ld(const T* p) { return *reinterpret_cast<const Lanes<T, V>*>(p); }
+template <typename T, int V>
+__device__ __forceinline__ void st(T* p, const Lanes<T, V>& a) { *reinterpret_cast<Lanes<T, V>*>(p) = a; }
+
+// Partial LU of a front held in registers (256 threads as 16 x 16; thread (r, c)
+// owns entries (r + 16 a, c + 16 b), a, b < TT, of its V lanes).  Per pivot the
+// owners publish column p (rows >= p) and row p (columns > p) to a shared buffer
+// (two buffers alternate, so one barrier per pivot suffices: a thread can only
+// reuse a buffer after passing the next pivot's barrier); every thread then
+// updates its own entries from the buffers.  Shared-memory traffic per pivot is
+// 2 TT values per thread for TT^2 multiply-adds, instead of a load and a store
+// of every updated entry.  Same operations per entry, in the same order, as the
+// shared-memory loop of k_mf_factor.  F: the assembled front; on return it holds
+// the factors (and the forward-substituted right-hand side column).
+template <typename T, int V, int TT>
+__device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int w, T* cbuf, T* rbuf, int fcap,
+                                             int* st_lanes, bool lead) {
+  using LV = Lanes<T, V>;
+  constexpr int G = V;
+  const int r = threadIdx.x & 15, c = threadIdx.x >> 4;
+  LV t[TT][TT];
+#pragma unroll
+  for (int a = 0; a < TT; ++a)
+#pragma unroll
+    for (int b = 0; b < TT; ++b) {
+      const int i = r + 16 * a, j = c + 16 * b;
+      if (i < f && j < ncols) t[a][b] = ld<T, V>(F + (i * RS + j) * G);
+      else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) t[a][b].v[k] = (T)0;
+      }
+    }
+  for (int p = 0; p < w; ++p) {
+    T* cp = cbuf + (p & 1) * fcap * G;        // column p, indexed by row
+    T* rp = rbuf + (p & 1) * (fcap + 1) * G;  // row p, indexed by column
+    const int pr = p & 15, pt = p >> 4;       // owners: thread row / column pr, tile index pt
+    if (c == pr) {
+#pragma unroll
+      for (int a = 0; a < TT; ++a)
+#pragma unroll
+        for (int b = 0; b < TT; ++b) {
+          const int i = r + 16 * a;
+          if (b == pt && i >= p && i < f) st<T, V>(cp + i * G, t[a][b]);
+        }
+    }
+    if (r == pr) {
+#pragma unroll
+      for (int a = 0; a < TT; ++a)
+#pragma unroll
+        for (int b = 0; b < TT; ++b) {
+          const int j = c + 16 * b;
+          if (a == pt && j > p && j < ncols) st<T, V>(rp + j * G, t[a][b]);
+        }
+    }
+    __syncthreads();
+    const LV piv = ld<T, V>(cp + p * G);
+    LV inv;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      T pk = piv.v[k];
+      if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
+        if (lead) st_lanes[k] = ST_SINGULAR;
+        pk = (T)1;
+      }
+      inv.v[k] = (T)1 / pk;
+    }
+    // row p's entries right of the pivot and the multipliers of the rows below it;
+    // zero elsewhere, so that the update leaves every other entry as it is (x - 0)
+    LV u[TT], l[TT];
+#pragma unroll
+    for (int b = 0; b < TT; ++b) {
+      const int j = c + 16 * b;
+      if (j > p && j < ncols) u[b] = ld<T, V>(rp + j * G);
+      else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) u[b].v[k] = (T)0;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < TT; ++a) {
+      const int i = r + 16 * a;
+      if (i > p && i < f) {
+        l[a] = ld<T, V>(cp + i * G);
+#pragma unroll
+        for (int k = 0; k < V; ++k) l[a].v[k] *= inv.v[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) l[a].v[k] = (T)0;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < TT; ++a)
+#pragma unroll
+      for (int b = 0; b < TT; ++b)
+#pragma unroll
+        for (int k = 0; k < V; ++k) t[a][b].v[k] = t[a][b].v[k] - l[a].v[k] * u[b].v[k];
+    if (c == pr) {
+#pragma unroll
+      for (int a = 0; a < TT; ++a)
+#pragma unroll
+        for (int b = 0; b < TT; ++b) {
+          const int i = r + 16 * a;
+          if (b == pt && i > p && i < f) t[a][b] = l[a];
+        }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < TT; ++a)
+#pragma unroll
+    for (int b = 0; b < TT; ++b) {
+      const int i = r + 16 * a, j = c + 16 * b;
+      if (i < f && j < ncols) st<T, V>(F + (i * RS + j) * G, t[a][b]);
+    }
+  __syncthreads();
+}
+
+// TT > 0: the partial LU runs in registers (lu_registers; TEAM 256 with one thread
+// per entry-lane group, i.e. G <= 16 bytes of lanes); TT = 0: in shared memory.
+template <typename T, int G, int TEAM, int TT = 0>
+__global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : 4) k_mf_factor(
     DevLU L, const int* __restrict__ task_sn, int nsn_l, int ngroups, int fcap,
     const T* __restrict__ A, T* __restrict__ pan, T* __restrict__ cb, T* __restrict__ cbr,
     T* __restrict__ x, int* __restrict__ status, const int* __restrict__ group_active, int with_rhs) {
-  constexpr int SLOTS = TEAM / G;
+  // a thread carries V adjacent lanes (16 bytes), NV threads cover the G lanes of a task
+  constexpr int V = (int)(16 / sizeof(T)) < G ? (int)(16 / sizeof(T)) : G;
+  constexpr int NV = G / V;
+  constexpr int SLOTS = TEAM / NV;
   constexpr int LPG = 32 / G;  // lane chunks per group
-  // slots of a lane form RSL row slots x CG column groups: rows are dealt to the
-  // row slots, and each column group takes a contiguous share of a row's columns
-  // (fronts have fewer rows than a 256-thread team has slots when G is small)
+  // slots form RSL row slots x CG column groups: rows are dealt to the row slots,
+  // and each column group takes a contiguous share of a row's columns (fronts have
+  // fewer rows than a 256-thread team has slots)
   constexpr int RSL = SLOTS < 32 ? SLOTS : 32;
   constexpr int CG = SLOTS / RSL;
-  constexpr int U = 8;  // loads issued before the dependent shared-memory stores
+  constexpr int U = V * sizeof(T) >= 16 ? 4 : 8;  // entries loaded before the dependent shared-memory stores
+  using LV = Lanes<T, V>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int teams = blockDim.x / TEAM;
   const int team = threadIdx.x / TEAM, tid = threadIdx.x % TEAM;
-  const int slot = tid / G, l = tid % G;
+  const int slot = tid / NV, lv = (tid % NV) * V;
   const int rs = slot % RSL, cg = slot / RSL;
-  T* F = reinterpret_cast<T*>(smem_raw) + (size_t)team * fcap * front_stride(fcap) * G;
+  T* F = reinterpret_cast<T*>(smem_raw) + (size_t)team * fcap * front_stride(fcap) * G + lv;
   const long long nchunks = (long long)ngroups * LPG;
   const long long ntasks = (long long)nsn_l * nchunks;
   for (long long t = (long long)blockIdx.x * teams + team; t < ntasks; t += (long long)gridDim.x * teams) {
@@ -496,118 +624,183 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM) k_mf_factor(
     const int ch = (int)(t % nchunks);
     const int g = ch / LPG;
     if (!group_active[g]) continue;
-    const int lane = (ch % LPG) * G + l;
+    const int lane = (ch % LPG) * G + lv;  // first of this thread's V lanes
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     const int RS = front_stride(f);
     const int ncols = with_rhs ? f + 1 : f;
-#define FR(r, c) F[((r) * RS + (c)) * G + l]
-    for (int idx = slot; idx < f * RS; idx += SLOTS) F[idx * G + l] = (T)0;
+    // F + (r * RS + c) * G: entry (r, c) of this thread's lanes
+#define FP(r, c) (F + ((r) * RS + (c)) * G)
+    {
+      LV z;
+#pragma unroll
+      for (int k = 0; k < V; ++k) z.v[k] = (T)0;
+      for (int idx = slot; idx < f * RS; idx += SLOTS) st<T, V>(F + idx * G, z);
+    }
     team_sync<TEAM>();
-    for (int e = L.ah_ptr[s] + slot; e < L.ah_ptr[s + 1]; e += SLOTS) F[L.ah_loc[e] * G + l] = A[at32(g, L.nA, e, lane)];
+    {
+      const T* a0 = A + at32(g, L.nA, 0, lane);
+      for (int e = L.ah_ptr[s] + slot; e < L.ah_ptr[s + 1]; e += SLOTS)
+        st<T, V>(F + L.ah_loc[e] * G, ld<T, V>(a0 + (size_t)e * 32));
+    }
     if (with_rhs)
-      for (int p = slot; p < w; p += SLOTS) FR(p, f) = x[at32(g, L.n, rows[p], lane)];
+      for (int p = slot; p < w; p += SLOTS) st<T, V>(FP(p, f), ld<T, V>(x + at32(g, L.n, rows[p], lane)));
     team_sync<TEAM>();
     for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
       const int ch2 = L.child_list[ci];
       const int m = L.sn_f[ch2] - L.sn_w[ch2];
       const int* rel = L.relmap + L.rel_ptr[ch2];
       const long long cbo = L.cb_off[ch2];
-      // column share of this column group
       const int b0 = (m * cg) / CG, b1 = (m * (cg + 1)) / CG;
       for (int a = rs; a < m; a += RSL) {
-        T* dst = &FR(rel[a], 0);
+        T* dst = FP(rel[a], 0);
         const T* src = cb + at32(g, L.sumcb, cbo + (long long)a * m, lane);
         int b = b0;
         for (; b + U <= b1; b += U) {
           int rb[U];
-          T v[U], o[U];
+          LV v[U], o[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             rb[u] = rel[b + u] * G;
-            v[u] = src[(size_t)(b + u) * 32];
+            v[u] = ld<T, V>(src + (size_t)(b + u) * 32);
           }
           // rel is injective: the U destinations are distinct
 #pragma unroll
-          for (int u = 0; u < U; ++u) o[u] = dst[rb[u]];
+          for (int u = 0; u < U; ++u) o[u] = ld<T, V>(dst + rb[u]);
 #pragma unroll
-          for (int u = 0; u < U; ++u) dst[rb[u]] = o[u] + v[u];
+          for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int k = 0; k < V; ++k) o[u].v[k] += v[u].v[k];
+            st<T, V>(dst + rb[u], o[u]);
+          }
         }
-        for (; b < b1; ++b) dst[rel[b] * G] += src[(size_t)b * 32];
-        if (with_rhs && cg == 0) FR(rel[a], f) += cbr[at32(g, L.sumcbr, L.cbr_off[ch2] + a, lane)];
+        for (; b < b1; ++b) {
+          T* d = dst + rel[b] * G;
+          LV o = ld<T, V>(d);
+          const LV v = ld<T, V>(src + (size_t)b * 32);
+#pragma unroll
+          for (int k = 0; k < V; ++k) o.v[k] += v.v[k];
+          st<T, V>(d, o);
+        }
+        if (with_rhs && cg == 0) {
+          T* d = FP(rel[a], f);
+          LV o = ld<T, V>(d);
+          const LV v = ld<T, V>(cbr + at32(g, L.sumcbr, L.cbr_off[ch2] + a, lane));
+#pragma unroll
+          for (int k = 0; k < V; ++k) o.v[k] += v.v[k];
+          st<T, V>(d, o);
+        }
       }
       team_sync<TEAM>();
     }
+    if constexpr (TT > 0) {
+      static_assert(TEAM == 256 && NV == 1, "register LU: one 256-thread team, one thread per entry");
+      T* bufs = reinterpret_cast<T*>(smem_raw) + (size_t)fcap * front_stride(fcap) * G;
+      lu_registers<T, V, TT>(F, RS, f, ncols, w, bufs, bufs + 2 * (size_t)fcap * G, fcap, status + g * 32 + lane,
+                             tid == 0);
+    } else {
     // Right-looking partial LU of the w pivots, one team barrier per pivot.  At
     // pivot p every thread reads the unscaled column p (l_ip = F(i,p) / F(p,p));
     // the scaled values are written back one pivot later, when no thread reads
     // column p any more (and after the loop for the last pivot).
-    T inv_prev = (T)0;
+    LV inv_prev;
     for (int p = 0; p < w; ++p) {
-      T piv = FR(p, p);
-      if (!(fabs((double)piv) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)piv) <= DBL_MAX)) {
-        if (slot == 0) status[g * 32 + lane] = ST_SINGULAR;
-        piv = (T)1;
+      const LV piv = ld<T, V>(FP(p, p));
+      LV inv;
+#pragma unroll
+      for (int k = 0; k < V; ++k) {
+        T pk = piv.v[k];
+        if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
+          if (slot == 0) status[g * 32 + lane + k] = ST_SINGULAR;
+          pk = (T)1;
+        }
+        inv.v[k] = (T)1 / pk;
       }
-      const T inv = (T)1 / piv;
       if (p > 0 && cg == CG - 1)
-        for (int i = p + rs; i < f; i += RSL) FR(i, p - 1) *= inv_prev;
+        for (int i = p + rs; i < f; i += RSL) {
+          LV c = ld<T, V>(FP(i, p - 1));
+#pragma unroll
+          for (int k = 0; k < V; ++k) c.v[k] *= inv_prev.v[k];
+          st<T, V>(FP(i, p - 1), c);
+        }
       const int nq = ncols - (p + 1);
       const int q0 = p + 1 + (nq * cg) / CG, q1 = p + 1 + (nq * (cg + 1)) / CG;
-      const T* rp = &FR(p, 0);
+      const T* rp = FP(p, 0);
       for (int i = p + 1 + rs; i < f; i += RSL) {
-        T* ri = &FR(i, 0);
-        const T lip = ri[p * G] * inv;
+        T* ri = FP(i, 0);
+        LV lip = ld<T, V>(ri + p * G);
+#pragma unroll
+        for (int k = 0; k < V; ++k) lip.v[k] *= inv.v[k];
         int q = q0;
         for (; q + U <= q1; q += U) {
-          T a[U], b[U];
+          LV a[U], b[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
-            a[u] = rp[(q + u) * G];
-            b[u] = ri[(q + u) * G];
+            a[u] = ld<T, V>(rp + (q + u) * G);
+            b[u] = ld<T, V>(ri + (q + u) * G);
           }
 #pragma unroll
-          for (int u = 0; u < U; ++u) ri[(q + u) * G] = b[u] - lip * a[u];
+          for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int k = 0; k < V; ++k) b[u].v[k] = b[u].v[k] - lip.v[k] * a[u].v[k];
+            st<T, V>(ri + (q + u) * G, b[u]);
+          }
         }
-        for (; q < q1; ++q) ri[q * G] -= lip * rp[q * G];
+        for (; q < q1; ++q) {
+          const LV a = ld<T, V>(rp + q * G);
+          LV b = ld<T, V>(ri + q * G);
+#pragma unroll
+          for (int k = 0; k < V; ++k) b.v[k] = b.v[k] - lip.v[k] * a.v[k];
+          st<T, V>(ri + q * G, b);
+        }
       }
       inv_prev = inv;
       team_sync<TEAM>();
     }
     if (w > 0) {
       if (cg == CG - 1)
-        for (int i = w + rs; i < f; i += RSL) FR(i, w - 1) *= inv_prev;
+        for (int i = w + rs; i < f; i += RSL) {
+          LV c = ld<T, V>(FP(i, w - 1));
+#pragma unroll
+          for (int k = 0; k < V; ++k) c.v[k] *= inv_prev.v[k];
+          st<T, V>(FP(i, w - 1), c);
+        }
       team_sync<TEAM>();
     }
+    }
     const long long po = L.pan_off[s];
+    T* pbase = pan + at32(g, L.nnz, po, lane);
     // U-panel: rows 0..w-1, all f columns; L-panel: rows w..f-1, columns 0..w-1
     {
       const int c0 = (f * cg) / CG, c1 = (f * (cg + 1)) / CG;
       for (int p = rs; p < w; p += RSL) {
-        T* dst = pan + at32(g, L.nnz, po + (long long)p * f, lane);
-        for (int q = c0; q < c1; ++q) dst[(size_t)q * 32] = FR(p, q);
+        T* dst = pbase + (size_t)p * f * 32;
+        const T* src = FP(p, 0);
+        for (int q = c0; q < c1; ++q) st<T, V>(dst + (size_t)q * 32, ld<T, V>(src + q * G));
       }
     }
     const int m = f - w;
     {
       const int c0 = (w * cg) / CG, c1 = (w * (cg + 1)) / CG;
       for (int i = rs; i < m; i += RSL) {
-        T* dst = pan + at32(g, L.nnz, po + (long long)w * f + (long long)i * w, lane);
-        for (int q = c0; q < c1; ++q) dst[(size_t)q * 32] = FR(w + i, q);
+        T* dst = pbase + ((size_t)w * f + (size_t)i * w) * 32;
+        const T* src = FP(w + i, 0);
+        for (int q = c0; q < c1; ++q) st<T, V>(dst + (size_t)q * 32, ld<T, V>(src + q * G));
       }
     }
     if (with_rhs)
-      for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, rows[p], lane)] = FR(p, f);
+      for (int p = slot; p < w; p += SLOTS) st<T, V>(x + at32(g, L.n, rows[p], lane), ld<T, V>(FP(p, f)));
     if (L.sn_parent[s] >= 0) {
-      const long long cbo = L.cb_off[s];
+      T* cbase = cb + at32(g, L.sumcb, L.cb_off[s], lane);
       const int c0 = (m * cg) / CG, c1 = (m * (cg + 1)) / CG;
       for (int a = rs; a < m; a += RSL) {
-        T* dst = cb + at32(g, L.sumcb, cbo + (long long)a * m, lane);
-        for (int b = c0; b < c1; ++b) dst[(size_t)b * 32] = FR(w + a, w + b);
-        if (with_rhs && cg == 0) cbr[at32(g, L.sumcbr, L.cbr_off[s] + a, lane)] = FR(w + a, f);
+        T* dst = cbase + (size_t)a * m * 32;
+        const T* src = FP(w + a, w);
+        for (int b = c0; b < c1; ++b) st<T, V>(dst + (size_t)b * 32, ld<T, V>(src + b * G));
+        if (with_rhs && cg == 0) st<T, V>(cbr + at32(g, L.sumcbr, L.cbr_off[s] + a, lane), ld<T, V>(FP(w + a, f)));
       }
     }
-#undef FR
+#undef FP
     team_sync<TEAM>();
   }
 }
