@@ -43,7 +43,34 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cases", type=int, default=0,
                     help="solve only the first N cases per GPU (small runs for profiling; 0 = all)")
+    ap.add_argument("--profile-solve", choices=["mixed", "fp64"], default=None,
+                    help="profiling driver: warm-up solves (which also autotune), then exactly one solve "
+                         "of this precision between cudaProfilerStart/Stop (for ncu --profile-from-start "
+                         "off); prints that solve's kernel timing and exits")
     return ap.parse_args()
+
+
+def profile_solve(args):
+    import torch
+
+    import mapol_b200 as m
+
+    buses, branches, cases = m.workload(args.workload)
+    if args.cases:
+        cases = cases[:args.cases]
+    prec = m.MIXED if args.profile_solve == "mixed" else m.FP64
+    with m.PowerFlow(buses, branches) as pf:
+        pf.set_cases(cases)
+        for _ in range(max(1, args.warmup)):
+            pf.solve(m.NR, prec)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        pf.solve(m.NR, prec)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        res = pf.results()
+        return {"profile_solve": args.profile_solve, "cases": len(cases), "converged": int(res.converged.sum()),
+                "timing": pf.timing(), "stats": pf.stats()}
 
 
 # ------------------------------------------------------------------ clocks
@@ -101,6 +128,19 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def factor_traffic_per_case():
+    """DRAM bytes per case of one factorisation, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "dram_nr_mixed_9241bus_256cases.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("factor_dram_bytes_per_case:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def measured_peaks():
@@ -295,6 +335,8 @@ def run_ours(args, rank, world, local_rank):
 
     fams = {k: v for k, v in mixed["fam"].items() if k != "other_ms"}
     dom = max(fams, key=fams.get)
+    tpc = factor_traffic_per_case() if args.workload == WORKLOAD and dom == "factor_ms" else None
+    traffic = round(tpc * n_cases) if tpc else None
     # units processed per step by that family: Newton iterations summed over cases
     units = mixed["iters_sum"]
     achieved = alg_bytes(dom, 4) * units / (fams[dom] / 1e3) / 1e9
@@ -326,7 +368,11 @@ def run_ours(args, rank, world, local_rank):
         "mixed_over_plain": value / value_fp64,
         "mixed": {"converged": mixed["n_conv"], "iterations_hist": mixed["iters"], "max_mismatch": mixed["max_mis"]},
         "roofline": {"bound": "hbm", "kernel": dom.replace("_ms", ""), "achieved": round(achieved, 1),
-                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "traffic_unit": "DRAM bytes per factorisation of all cases (its 45 launches)",
+                     "alg_bytes": alg_bytes("factor_ms", 4) * n_cases,
+                     "traffic_source": "ncu dram__bytes_read+write.sum, 256 cases, per case x cases "
+                                       "(profiles/dram_nr_mixed_9241bus_256cases.md)",
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                      "per_family": per_family},
         "gpu_launches": int(mixed["launches"]),
@@ -347,6 +393,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(reference_arm(args)), flush=True)
+        return 0
+    if args.profile_solve:
+        print(json.dumps(profile_solve(args)), flush=True)
         return 0
     if world > 1:
         import datetime
