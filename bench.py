@@ -164,7 +164,7 @@ def cpu_port_baseline(buses, branches, cases, budget_s=15.0):
     dt = time.perf_counter() - t
     # grow the sample toward the time budget
     if dt < budget_s / 4 and n < len(cases):
-        n2 = min(len(cases), int(n * budget_s / 2 / max(dt, 1e-3)))
+        n2 = min(len(cases), int(n * budget_s / max(dt, 1e-3)))
         t = time.perf_counter()
         r = oracle.runpf(buses, branches, cases[:n2], alg=0, solver=oracle.SOLVER_GP, threads=threads)
         dt = time.perf_counter() - t

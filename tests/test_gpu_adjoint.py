@@ -134,3 +134,68 @@ def test_autograd_function_backward_is_the_adjoint(base):
         (out * w).sum().backward()
     np.testing.assert_allclose(p.grad.numpy(), g["grad_p"] * w.numpy()[:, None], rtol=1e-9, atol=1e-14)
     np.testing.assert_allclose(q.grad.numpy(), g["grad_q"] * w.numpy()[:, None], rtol=1e-9, atol=1e-14)
+
+
+def _explicit_loss(buses, branches, v, rating, outages):
+    """sum relu(|Sf| - 0.9 rating)^2 at complex voltages v (pi model, numpy)."""
+    br = branches
+    ys = np.where(br["status"] == 1, 1.0 / (br["r"] + 1j * br["x"]), 0.0)
+    bc = np.where(br["status"] == 1, br["b"], 0.0)
+    tap = np.where(br["tap"] != 0, br["tap"], 1.0) * np.exp(1j * np.pi / 180 * br["shift"])
+    yff = (ys + 0.5j * bc) / np.abs(tap) ** 2
+    yft = -ys / np.conj(tap)
+    vf, vt = v[br["from"]], v[br["to"]]
+    sf = vf * np.conj(yff * vf + yft * vt)
+    ex = np.abs(sf) - 0.9 * rating
+    on = np.ones(len(br), bool)
+    on[list(outages)] = False
+    return float(np.sum(np.where(on & (ex > 0), ex * ex, 0.0)))
+
+
+def test_adjoint_matches_dense_implicit_function_gradient(base):
+    """lambda = J^-T dL/dx with the oracle's Jacobian at the oracle's solution (dense
+    FP64 solve), dL/dx by central differences (step 1e-7) of the explicit loss: the
+    P/Q gradients agree with the adjoint to 1e-6 relative (2-norm over each case)."""
+    from oracle import oracle
+
+    buses, branches, cases, rating, L, g, _ = base
+    ref = oracle.runpf(buses, branches, cases, alg=0, tol=1e-12)
+    pv = np.where(buses["type"] == 2)[0]
+    pq = np.where(buses["type"] == 1)[0]
+    npv, npq = len(pv), len(pq)
+    checked = 0
+    for c, out in enumerate(cases):
+        if L[c] == 0.0:
+            continue
+        v = ref["v"][c]
+        _, (jp, jc, jv), _ = oracle.nr_system(buses, branches, v, outages=out)
+        n = npv + 2 * npq
+        J = np.zeros((n, n))
+        for r in range(n):
+            J[r, jc[jp[r]:jp[r + 1]]] = jv[jp[r]:jp[r + 1]]
+        # x = [Va (PV, PQ), Vm (PQ)], bus-index order within each group
+        va_bus = np.concatenate([pv, pq])
+        dldx = np.zeros(n)
+        h = 1e-7
+        for k in range(n):
+            vp, vm_ = v.copy(), v.copy()
+            if k < npv + npq:
+                i = va_bus[k]
+                vp[i] *= np.exp(1j * h)
+                vm_[i] *= np.exp(-1j * h)
+            else:
+                i = pq[k - npv - npq]
+                vp[i] *= (abs(v[i]) + h) / abs(v[i])
+                vm_[i] *= (abs(v[i]) - h) / abs(v[i])
+            dldx[k] = (_explicit_loss(buses, branches, vp, rating, out)
+                       - _explicit_loss(buses, branches, vm_, rating, out)) / (2 * h)
+        lam = np.linalg.solve(J.T, dldx)
+        gp = np.zeros(len(buses))
+        gq = np.zeros(len(buses))
+        gp[va_bus] = lam[:npv + npq]
+        gq[pq] = lam[npv + npq:]
+        a = np.concatenate([g["grad_p"][c], g["grad_q"][c]])
+        d = np.concatenate([gp, gq])
+        assert np.linalg.norm(a - d) <= 1e-6 * np.linalg.norm(d), (c, np.linalg.norm(a - d), np.linalg.norm(d))
+        checked += 1
+    assert checked >= 3
