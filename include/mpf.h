@@ -148,7 +148,9 @@ const char* mpf_status_string(int32_t status);
 /* ---- handle lifecycle (replaces hybrid_init / hybrid_free) ------------- */
 /* Validates the grid, builds the superset Ybus pattern, the Jacobian, B' and B''
  * patterns, their fill-reducing orderings and symbolic LU, and uploads the shared
- * (case-independent) arrays to the device.  Exactly one slack bus is required. */
+ * (case-independent) arrays to the device.  Every connected island with PV/PQ
+ * buses needs exactly one slack bus (one island per grid; several islands: see
+ * mpf_set_cases_islands). */
 int32_t mpf_create(const mpf_bus* buses, int32_t n_bus,
                    const mpf_branch* branches, int32_t n_branch,
                    const mpf_options* opt, mpf_handle** out);
@@ -166,6 +168,21 @@ int32_t mpf_get_stats(const mpf_handle* h, mpf_stats* st);
 int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases,
                       const int32_t* outage_offsets, const int32_t* outage_branches,
                       const double* sbus);
+
+/* Several grids in one batch.  A handle may hold several grids as the islands of
+ * one grid (concatenate their buses and branches with index offsets; each island,
+ * i.e. connected component, has exactly one slack bus; islands are numbered in the
+ * order of their slack buses).  Every Newton / fast-decoupled stage then runs all
+ * islands' cases in the same launches: the Jacobian is block-diagonal by island, each
+ * case belongs to one island, and rows, branches and supernodes of other islands are
+ * skipped.  mpf_set_cases takes a case's island from its outaged branches; this form
+ * gives island_of_case[n_cases] explicitly (required for cases without outages on a
+ * grid with several islands).  Results stay per case, over all buses / branches of
+ * the handle (entries of other islands hold the start point / zero).  No counterpart
+ * in the reference, which handles one grid per process (runpf.h:795). */
+int32_t mpf_set_cases_islands(mpf_handle* h, int32_t n_cases, const int32_t* island_of_case,
+                              const int32_t* outage_offsets, const int32_t* outage_branches,
+                              const double* sbus);
 
 /* Per-case control overrides: the optimiser's structures of
  * src/pso/Particula.h:26-60 (kinds keep the values of its enum Tipo), applied as

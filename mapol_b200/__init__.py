@@ -9,5 +9,6 @@ from ._types import (BRANCH_DTYPE, BUS_DTYPE, CTRL_AVR, CTRL_OLTC, CTRL_SHC, EPS
 from .grid import (find_bridges, load_scenarios, n1_cases, select_outages, synth_grid,  # noqa: F401
                    workload, WORKLOADS)
 from .runpf import PowerFlow, Results, hybrid_free, hybrid_init, hybrid_runpf  # noqa: F401
+from .multigrid import MultiGrid  # noqa: F401
 
 __version__ = "0.1.0"

@@ -101,6 +101,8 @@ struct LUSystem {
   LUSymbolic sym;
   DevBuf sn_w, sn_f, sn_rptr, sn_rows, child_ptr, child_list, sn_parent, rel_ptr, relmap, ah_ptr, ah_loc;
   DevBuf pan_off, cb_off, cbr_off, lev_sn;
+  DevBuf sn_island;                  // multi-island handles only
+  const int* group_island = nullptr; // the handle's current per-group islands (or null)
   std::vector<Launch> factor_sched;  // ascending levels
   // autotuned kernel of every factor_sched launch, per (precision, case groups)
   std::map<std::pair<int, int>, std::vector<FactorChoice>> tuned;
@@ -132,12 +134,26 @@ struct LUSystem {
     d.pan_off = pan_off.as<long long>();
     d.cb_off = cb_off.as<long long>();
     d.cbr_off = cbr_off.as<long long>();
+    d.sn_island = group_island ? sn_island.as<int>() : nullptr;
+    d.group_island = group_island;
     return d;
   }
 
-  void setup(const LUSymbolic& s, const std::vector<int>& ahp, const std::vector<int>& ahl, int nA_) {
+  // var_island (multi-island handles): island of each variable; a supernode's
+  // variables all belong to one island (the matrix is block-diagonal by island)
+  void setup(const LUSymbolic& s, const std::vector<int>& ahp, const std::vector<int>& ahl, int nA_,
+             const std::vector<int>* var_island = nullptr) {
     sym = s;
     nA = nA_;
+    if (var_island) {
+      std::vector<int> si(s.nsn);
+      for (int k = 0; k < s.nsn; ++k) {
+        si[k] = (*var_island)[s.sn_rows[s.sn_rptr[k]]];
+        for (int q = s.sn_rptr[k]; q < s.sn_rptr[k] + s.sn_w[k]; ++q)
+          if ((*var_island)[s.sn_rows[q]] != si[k]) throw MpfError{MPF_ERR_INTERNAL, "supernode spans two islands"};
+      }
+      upload(sn_island, si);
+    }
     upload(sn_w, s.sn_w);
     upload(sn_f, s.sn_f);
     upload(sn_rptr, s.sn_rptr);
@@ -605,6 +621,10 @@ struct mpf_handle {
   DevBuf eval_acc;  // mpf_mismatch accumulator, allocated on first use
   DevBuf br_dy;     // per branch dY/dg for (ff, ft, tf, tt), adjoint
   DevBuf adj_status;  // statuses the adjoint's refactorisation may write (kept apart)
+  // several islands (grids) in one handle: per-bus / per-branch islands, and per
+  // batch the island of each group and the case <-> lane maps
+  DevBuf bus_island, br_island, group_island, lane_case, case_lane;
+  std::vector<int> h_lane_case;
   std::vector<mpf_bus> buses;        // the grid as given (controls read base values)
   std::vector<mpf_branch> branches;
   // per-case controls of the current cases (mpf_set_controls)
@@ -677,6 +697,13 @@ struct mpf_handle {
     d.group_active = group_active.as<int>();
     d.any_active = any_active.as<int>();
     d.it_ptr = it_ctr.as<int>();
+    if (g.n_islands > 1 && group_island.p) {
+      d.bus_island = bus_island.as<int>();
+      d.br_island = br_island.as<int>();
+      d.group_island = group_island.as<int>();
+      d.lane_case = lane_case.as<int>();
+      d.case_lane = case_lane.as<int>();
+    }
     if (ctl.nc > 0) {
       d.nslot = ctl.nslot;
       d.noltc = ctl.noltc;
@@ -717,7 +744,7 @@ struct mpf_handle {
     const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &y_diag, &br_ft, &rating, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
                            &out_br, &sbus_case, &V, &Ibus, &status, &iters, &maxmis, &facc, &group_active,
                            &any_active, &vout, &small_out, &fdvar, &eval_acc, &it_ctr, &br_dy,
-                           &adj_status};
+                           &adj_status, &bus_island, &br_island, &group_island, &lane_case, &case_lane};
     for (auto p : all) b += p->bytes;
     b += ctl.bytes();
     const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
@@ -758,7 +785,14 @@ void upload_fd(mpf_handle* h, int variant) {
   if (h->fd_ready[variant]) return;
   const GridSymbolic& g = h->g;
   auto setup_one = [&](const GridSymbolic::FDSystem& fs, LUSystem& sys, FDData& fd) {
-    sys.setup(fs.lu, fs.ah_ptr, fs.ah_loc, (int)fs.base.size());
+    std::vector<int> vi;
+    if (g.n_islands > 1) {
+      vi.assign(fs.lu.n, -1);
+      for (int i = 0; i < g.nb; ++i)
+        if (fs.var[i] >= 0) vi[fs.var[i]] = g.bus_island[i];
+    }
+    sys.setup(fs.lu, fs.ah_ptr, fs.ah_loc, (int)fs.base.size(), g.n_islands > 1 ? &vi : nullptr);
+    sys.group_island = h->jac.group_island;
     upload(fd.base, fs.base);
     std::vector<int4> pos(g.nbr);
     std::vector<double4> val(g.nbr);
@@ -1239,7 +1273,18 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
         jp[p] = make_int4(g.jpos[4 * p], g.jpos[4 * p + 1], g.jpos[4 * p + 2], g.jpos[4 * p + 3]);
       upload(h->jpos, jp);
     }
-    h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac);
+    if (g.n_islands > 1) {
+      std::vector<int> vi(g.jac.n, -1);
+      for (int i = 0; i < g.nb; ++i) {
+        if (g.var_va[i] >= 0) vi[g.var_va[i]] = g.bus_island[i];
+        if (g.var_vm[i] >= 0) vi[g.var_vm[i]] = g.bus_island[i];
+      }
+      h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac, &vi);
+      upload(h->bus_island, g.bus_island);
+      upload(h->br_island, g.br_island);
+    } else {
+      h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac);
+    }
     h->any_active.alloc(sizeof(int));
     h->it_ctr.alloc(sizeof(int));
     return MPF_OK;
@@ -1271,7 +1316,7 @@ int32_t mpf_get_stats(const mpf_handle* h, mpf_stats* st) {
   st->n_branch = g.nbr;
   st->n_pv = g.npv;
   st->n_pq = g.npq;
-  st->n_slack = g.slack >= 0 ? 1 : 0;
+  st->n_slack = g.n_slack;
   st->nnz_ybus = g.y_rowptr.empty() ? 0 : g.y_rowptr.back();
   st->n_jac = g.jac.n;
   st->nnz_jac = g.nnz_jac;
@@ -1290,8 +1335,25 @@ int32_t mpf_get_stats(const mpf_handle* h, mpf_stats* st) {
   return MPF_OK;
 }
 
+namespace {
+int set_cases_impl(mpf_handle* h, int32_t n_cases, const int32_t* island_of_case, const int32_t* outage_offsets,
+                   const int32_t* outage_branches, const double* sbus);
+}  // namespace
+
 int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases, const int32_t* outage_offsets, const int32_t* outage_branches,
                       const double* sbus) {
+  return set_cases_impl(h, n_cases, nullptr, outage_offsets, outage_branches, sbus);
+}
+
+int32_t mpf_set_cases_islands(mpf_handle* h, int32_t n_cases, const int32_t* island_of_case,
+                              const int32_t* outage_offsets, const int32_t* outage_branches, const double* sbus) {
+  if (h && !island_of_case) return fail(h, MPF_ERR_BAD_INPUT, "island_of_case is required");
+  return set_cases_impl(h, n_cases, island_of_case, outage_offsets, outage_branches, sbus);
+}
+
+namespace {
+int set_cases_impl(mpf_handle* h, int32_t n_cases, const int32_t* island_of_case, const int32_t* outage_offsets,
+                   const int32_t* outage_branches, const double* sbus) {
   if (!h) return MPF_ERR_BAD_INPUT;
   if (n_cases < 1) return fail(h, MPF_ERR_BAD_INPUT, "n_cases must be >= 1");
   if ((outage_offsets == nullptr) != (outage_branches == nullptr) && outage_offsets && outage_offsets[n_cases] > 0)
@@ -1302,12 +1364,50 @@ int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases, const int32_t* outage_offs
     CUDA_TRY(cudaStreamSynchronize(h->own_stream));
     if (h->last_stream) CUDA_TRY(cudaStreamSynchronize(h->last_stream));
     const GridSymbolic& g = h->g;
-    const int ngroups = (n_cases + 31) / 32;
+    const bool multi = g.n_islands > 1;
+    if (outage_offsets && outage_offsets[0] != 0) return fail(h, MPF_ERR_BAD_INPUT, "outage_offsets[0] must be 0");
+    // island of each case; lanes grouped by island, each island padded to whole groups
+    std::vector<int> island(n_cases, 0);
+    for (int c = 0; c < n_cases; ++c) {
+      const bool has_out = outage_offsets && outage_offsets[c + 1] > outage_offsets[c];
+      if (island_of_case) {
+        if (island_of_case[c] < 0 || island_of_case[c] >= g.n_islands)
+          return fail(h, MPF_ERR_BAD_INPUT, "case " + std::to_string(c) + ": island out of range");
+        island[c] = island_of_case[c];
+      } else if (multi) {
+        if (!has_out)
+          return fail(h, MPF_ERR_BAD_INPUT, "case " + std::to_string(c) + " has no outage to tell its island: "
+                                            "use mpf_set_cases_islands on a grid with several islands");
+        const int br = outage_branches[outage_offsets[c]];
+        if (br < 0 || br >= g.nbr)
+          return fail(h, MPF_ERR_BAD_INPUT, "case " + std::to_string(c) + ": outaged branch index out of range");
+        island[c] = g.br_island[br];
+      }
+    }
+    std::vector<int> case_lane(n_cases), lane_case, group_island;
+    int ngroups = 0;
+    if (multi) {
+      std::vector<int> count(g.n_islands, 0), next(g.n_islands, 0);
+      for (int c = 0; c < n_cases; ++c) ++count[island[c]];
+      for (int k = 0; k < g.n_islands; ++k) {
+        next[k] = ngroups * 32;
+        const int gk = (count[k] + 31) / 32;
+        for (int q = 0; q < gk; ++q) group_island.push_back(k);
+        ngroups += gk;
+      }
+      lane_case.assign((size_t)ngroups * 32, -1);
+      for (int c = 0; c < n_cases; ++c) {
+        case_lane[c] = next[island[c]]++;
+        lane_case[case_lane[c]] = c;
+      }
+    } else {
+      ngroups = (n_cases + 31) / 32;
+      for (int c = 0; c < n_cases; ++c) case_lane[c] = c;
+    }
     const int lanes = ngroups * 32;
     std::vector<int> outs((size_t)kMaxOut * lanes, -1);
     int maxk = 0;
     if (outage_offsets) {
-      if (outage_offsets[0] != 0) return fail(h, MPF_ERR_BAD_INPUT, "outage_offsets[0] must be 0");
       for (int c = 0; c < n_cases; ++c) {
         const int b = outage_offsets[c], e = outage_offsets[c + 1];
         if (e < b) return fail(h, MPF_ERR_BAD_INPUT, "outage_offsets must be non-decreasing");
@@ -1321,7 +1421,9 @@ int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases, const int32_t* outage_offs
           for (int k2 = b; k2 < k; ++k2)
             if (outage_branches[k2] == br)
               return fail(h, MPF_ERR_BAD_INPUT, "case " + std::to_string(c) + " lists a branch twice");
-          outs[(size_t)(k - b) * lanes + c] = br;
+          if (multi && g.br_island[br] != island[c])
+            return fail(h, MPF_ERR_BAD_INPUT, "case " + std::to_string(c) + " outages a branch of another island");
+          outs[(size_t)(k - b) * lanes + case_lane[c]] = br;
         }
         maxk = std::max(maxk, e - b);
       }
@@ -1334,7 +1436,8 @@ int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases, const int32_t* outage_offs
           const double p = sbus[((size_t)c * g.nb + i) * 2], q = sbus[((size_t)c * g.nb + i) * 2 + 1];
           if (!std::isfinite(p) || !std::isfinite(q))
             return fail(h, MPF_ERR_BAD_INPUT, "sbus has a non-finite value");
-          sb[((size_t)(c >> 5) * g.nb + i) * 32 + (c & 31)] = make_double2(p, q);
+          const int ln = case_lane[c];
+          sb[((size_t)(ln >> 5) * g.nb + i) * 32 + (ln & 31)] = make_double2(p, q);
         }
     }
     if (ngroups != h->ngroups) {
@@ -1357,6 +1460,18 @@ int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases, const int32_t* outage_offs
     upload(h->out_br, outs);
     if (sbus) upload(h->sbus_case, sb);
     else h->sbus_case.release();
+    if (multi) {
+      upload(h->group_island, group_island);
+      upload(h->lane_case, lane_case);
+      upload(h->case_lane, case_lane);
+    }
+    h->h_lane_case = lane_case;
+    const int* gi = multi ? h->group_island.as<int>() : nullptr;
+    h->jac.group_island = gi;
+    for (int v = 0; v < 2; ++v) {
+      h->bp[v].group_island = gi;
+      h->bpp[v].group_island = gi;
+    }
     h->ncases = n_cases;
     h->ngroups = ngroups;
     h->maxk = maxk;
@@ -1366,6 +1481,7 @@ int32_t mpf_set_cases(mpf_handle* h, int32_t n_cases, const int32_t* outage_offs
     return MPF_OK;
   });
 }
+}  // namespace
 
 int32_t mpf_set_controls(mpf_handle* h, int32_t n_controls, const mpf_control* controls, const double* values) {
   if (!h) return MPF_ERR_BAD_INPUT;
@@ -1415,7 +1531,8 @@ int32_t mpf_set_controls(mpf_handle* h, int32_t n_controls, const mpf_control* c
     std::vector<double> val((size_t)h->ngroups * nc * 32);
     for (int c = 0; c < lanes; ++c)
       for (int k = 0; k < nc; ++k) {
-        const double v = c < ncases ? values[(size_t)c * nc + k] : base[k];
+        const int uc = h->h_lane_case.empty() ? (c < ncases ? c : -1) : h->h_lane_case[c];
+        const double v = uc >= 0 ? values[(size_t)uc * nc + k] : base[k];
         if (!std::isfinite(v)) return fail(h, MPF_ERR_BAD_INPUT, "control values must be finite");
         if (controls[k].kind != MPF_CTRL_SHC && !(v > 0.0))
           return fail(h, MPF_ERR_BAD_INPUT, "AVR and OLTC values must be > 0");
@@ -1574,12 +1691,13 @@ int32_t mpf_get_results_device(mpf_handle* h, double* v, int32_t* iterations, ui
     if (v) {
       const size_t total = (size_t)h->ncases * h->g.nb;
       k_gather_v<<<(unsigned)std::min<size_t>(148 * 16, total / 256 + 1), 256, 0, st>>>(
-          h->g.nb, h->ncases, h->V.as<double2>(), reinterpret_cast<double2*>(v));
+          h->g.nb, h->ncases, h->dev().case_lane, h->V.as<double2>(), reinterpret_cast<double2*>(v));
       CUDA_TRY(cudaGetLastError());
     }
     if (iterations || status || max_mis) {
-      k_gather_small<<<(h->ncases + 255) / 256, 256, 0, st>>>(h->ncases, h->status.as<int>(), h->iters.as<int>(),
-                                                             h->maxmis.as<double>(), status, iterations, max_mis);
+      k_gather_small<<<(h->ncases + 255) / 256, 256, 0, st>>>(h->ncases, h->dev().case_lane, h->status.as<int>(),
+                                                             h->iters.as<int>(), h->maxmis.as<double>(), status,
+                                                             iterations, max_mis);
       CUDA_TRY(cudaGetLastError());
     }
     return MPF_OK;

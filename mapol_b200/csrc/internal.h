@@ -105,7 +105,10 @@ std::vector<int> minimum_degree(int n, const std::vector<std::vector<int>>& adj)
 
 // Everything that does not depend on the case batch.
 struct GridSymbolic {
-  int nb = 0, nbr = 0, npv = 0, npq = 0, slack = -1;
+  int nb = 0, nbr = 0, npv = 0, npq = 0, slack = -1, n_slack = 0;
+  int n_islands = 0;                 // connected islands with a slack (grids of a multi-grid handle)
+  std::vector<int> bus_island;       // per bus: island, -1 for buses of slack-less islands without equations
+  std::vector<int> br_island;        // per branch: island of its buses
   std::vector<int> pv, pq;           // bus-index order (Topology.h:100-126)
   std::vector<int> bus_type;
   // Ybus superset pattern (every branch, in or out of service), CSR, columns sorted

@@ -69,7 +69,26 @@ struct DevGrid {
   const int* br_ctl;        // [nbr] index among the controlled taps or -1
   const double2* ctl_bry;   // [g][4 noltc][32] admittances (ff, ft, tf, tt) of the controlled taps
   const double2* ctl_bdy;   // [g][4 noltc][32] their dY/dg (adjoint)
+  // several islands (multi-grid handle; null for one): a group's lanes all belong to
+  // one island, and rows, branches and supernodes of other islands are skipped
+  const int* bus_island;    // [nb]
+  const int* br_island;     // [nbr]
+  const int* group_island;  // [ngroups]
+  // case <-> lane when lanes are grouped by island and padded (null: lane = case)
+  const int* lane_case;     // [ngroups*32] user case or -1 (padding)
+  const int* case_lane;     // [ncases]
 };
+
+__device__ __forceinline__ bool row_here(const DevGrid& d, int i, int g) {
+  return !d.group_island || d.bus_island[i] == d.group_island[g];
+}
+__device__ __forceinline__ bool branch_here(const DevGrid& d, int k, int g) {
+  return !d.group_island || d.br_island[k] == d.group_island[g];
+}
+__device__ __forceinline__ int lane_of_case(const DevGrid& d, int c) { return d.case_lane ? d.case_lane[c] : c; }
+__device__ __forceinline__ int case_of_lane(const DevGrid& d, int lane, int ncases) {
+  return d.lane_case ? d.lane_case[lane] : (lane < ncases ? lane : -1);
+}
 
 struct DevLU {
   int n, nsn, nA;
@@ -88,7 +107,13 @@ struct DevLU {
   const long long* pan_off;
   const long long* cb_off;
   const long long* cbr_off;
+  const int* sn_island;     // [nsn] island of each supernode (null: one island)
+  const int* group_island;  // [ngroups]
 };
+
+__device__ __forceinline__ bool task_here(const DevLU& L, int s, int g) {
+  return !L.sn_island || L.sn_island[s] == L.group_island[g];
+}
 
 // ---------------------------------------------------------------- helpers
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -211,7 +236,7 @@ __global__ void k_init(DevGrid d, int ncases) {
   }
   const int nl = d.ngroups * 32;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nl; c += gridDim.x * blockDim.x) {
-    d.status[c] = c < ncases ? ST_RUNNING : ST_CONVERGED;
+    d.status[c] = case_of_lane(d, c, ncases) >= 0 ? ST_RUNNING : ST_CONVERGED;
     d.iters[c] = 0;
     d.maxmis[c] = 0.0;
     d.facc[c] = 0ull;
@@ -272,6 +297,7 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
   const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
   for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
     const int i = d.mis_rows[r];
+    if (!row_here(d, i, g)) continue;
     double2 ib = make_double2(0.0, 0.0);
     const int p0 = d.y_rowptr[i], p1 = d.y_rowptr[i + 1];
     const bool touched = row_touched(o, d.y_diag[i]);
@@ -335,6 +361,7 @@ __global__ void __launch_bounds__(256) k_update_nr(DevGrid d, const T* x) {
   const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
   for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
     const int i = d.mis_rows[r];
+    if (!row_here(d, i, g)) continue;
     const int2 jv = d.jvar[i];
     const double dva = (double)x[at32(g, d.n_jac, jv.x, lane)];
     const double dvm = jv.y >= 0 ? (double)x[at32(g, d.n_jac, jv.y, lane)] : 0.0;
@@ -367,6 +394,7 @@ __global__ void __launch_bounds__(256) k_mismatch_fd(DevGrid d, DevFD f, T* xp, 
   const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
   for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
     const int i = d.mis_rows[r];
+    if (!row_here(d, i, g)) continue;
     double2 ib = make_double2(0.0, 0.0);
     const bool touched = row_touched(o, d.y_diag[i]);
     for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
@@ -405,6 +433,7 @@ __global__ void __launch_bounds__(256) k_update_fd(DevGrid d, DevFD f, const T* 
   const int r1 = min(d.nfree, (blockIdx.x + 1) * kRowsPerBlock);
   for (int r = blockIdx.x * kRowsPerBlock + warp; r < r1; r += 8) {
     const int i = d.mis_rows[r];
+    if (!row_here(d, i, g)) continue;
     const int2 fv = f.fdvar[i];
     if (half == 1 && fv.y < 0) continue;
     const size_t k = at32(g, d.nb, i, lane);
@@ -623,7 +652,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : 4) k_mf_
     const int s = task_sn[t / nchunks];
     const int ch = (int)(t % nchunks);
     const int g = ch / LPG;
-    if (!group_active[g]) continue;
+    if (!group_active[g] || !task_here(L, s, g)) continue;
     const int lane = (ch % LPG) * G + lv;  // first of this thread's V lanes
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
@@ -819,7 +848,7 @@ __global__ void __launch_bounds__(128) k_mf_fsolve(DevLU L, const int* __restric
   for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
     const int s = task_sn[t / ngroups];
     const int g = (int)(t % ngroups);
-    if (!group_active[g]) continue;
+    if (!group_active[g] || !task_here(L, s, g)) continue;
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     for (int i = 0; i < f; ++i) b[i * 32 + lane] = (T)0;
@@ -860,7 +889,7 @@ __global__ void __launch_bounds__(128) k_mf_bsolve(DevLU L, const int* __restric
   for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
     const int s = task_sn[t / ngroups];
     const int g = (int)(t % ngroups);
-    if (!group_active[g]) continue;
+    if (!group_active[g] || !task_here(L, s, g)) continue;
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     const long long po = L.pan_off[s];
@@ -901,7 +930,7 @@ __global__ void __launch_bounds__(128) k_mf_bsolve_chunk(DevLU L, const int* __r
     const int s = task_sn[t / nchunks];
     const int ch = (int)(t % nchunks);
     const int g = ch / LPG;
-    if (!group_active[g]) continue;
+    if (!group_active[g] || !task_here(L, s, g)) continue;
     const int lane = (ch % LPG) * G + l;
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
@@ -930,25 +959,26 @@ __global__ void __launch_bounds__(128) k_mf_bsolve_chunk(DevLU L, const int* __r
 // folds them with shuffles, then one atomicMax per warp into acc[c].
 __global__ void __launch_bounds__(256) k_mismatch_eval(DevGrid d, const double2* __restrict__ v, int ncases,
                                                        unsigned long long* __restrict__ acc) {
-  const int c = blockIdx.y;
+  const int c = blockIdx.y;  // the user's case; its lane is ln
   if (c >= ncases) return;
+  const int ln = lane_of_case(d, c);
   LaneOut o;
-  load_outages(d, c, o);
+  load_outages(d, ln, o);
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   double m = 0.0;
-  if (r < d.nfree) {
+  if (r < d.nfree && row_here(d, d.mis_rows[r], ln >> 5)) {
     const double2* vc = v + (size_t)c * d.nb;
     const int i = d.mis_rows[r];
     double2 ib = make_double2(0.0, 0.0);
     const bool touched = row_touched(o, d.y_diag[i]);
     for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
-      const double2 y = yentry(d, o, touched, p, c >> 5, c & 31);
+      const double2 y = yentry(d, o, touched, p, ln >> 5, ln & 31);
       const double2 vj = vc[d.y_col[p]];
       ib.x += y.x * vj.x - y.y * vj.y;
       ib.y += y.x * vj.y + y.y * vj.x;
     }
     const double2 vi = vc[i];
-    const double2 s = d.sbus_case ? d.sbus_case[at32(c >> 5, d.nb, i, c & 31)] : d.sbus0[i];
+    const double2 s = d.sbus_case ? d.sbus_case[at32(ln >> 5, d.nb, i, ln & 31)] : d.sbus0[i];
     const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
     const double mi = vi.y * ib.x - vi.x * ib.y - s.y;
     m = fabs(mr);
@@ -984,6 +1014,7 @@ __global__ void __launch_bounds__(256) k_branch_flow(DevGrid d, int nbr, int nca
   const int g = blockIdx.y;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int c = g * 32 + lane;
+  const int uc = case_of_lane(d, c, ncases);  // the user's case in this lane, -1 for padding
   LaneOut o;
   load_outages(d, c, o);
   double lsum = 0.0, osum = 0.0;
@@ -991,7 +1022,8 @@ __global__ void __launch_bounds__(256) k_branch_flow(DevGrid d, int nbr, int nca
   const int k1 = min(nbr, k0 + 64);
   for (int k = k0 + warp; k < k1; k += 8) {
     double2 sf = make_double2(0.0, 0.0), stt = make_double2(0.0, 0.0);
-    if (!outaged(o, k)) {
+    const bool here = branch_here(d, k, g);
+    if (here && !outaged(o, k)) {
       const int2 ft = d.br_ft[k];
       double2 y[4];
       branch_y(d, k, g, lane, y);
@@ -1004,28 +1036,28 @@ __global__ void __launch_bounds__(256) k_branch_flow(DevGrid d, int nbr, int nca
       stt = make_double2(vt.x * i_t.x + vt.y * i_t.y, vt.y * i_t.x - vt.x * i_t.y);
     }
     lsum += sf.x + stt.x;
-    if (rating) {
+    if (rating && here) {
       const double ex = sqrt(sf.x * sf.x + sf.y * sf.y) - 0.9 * rating[k];
       if (ex > 0.0) osum += ex * ex;
     }
-    if (c < ncases) {
-      if (sf_out) sf_out[(size_t)c * nbr + k] = sf;
-      if (st_out) st_out[(size_t)c * nbr + k] = stt;
+    if (uc >= 0) {
+      if (sf_out) sf_out[(size_t)uc * nbr + k] = sf;
+      if (st_out) st_out[(size_t)uc * nbr + k] = stt;
     }
   }
   __shared__ double red[2][8][32];
   red[0][warp][lane] = lsum;
   red[1][warp][lane] = osum;
   __syncthreads();
-  if (warp == 0 && c < ncases) {
+  if (warp == 0 && uc >= 0) {
     double a = 0.0, b = 0.0;
 #pragma unroll
     for (int w = 0; w < 8; ++w) {
       a += red[0][w][lane];
       b += red[1][w][lane];
     }
-    atomicAdd(&ploss[c], a);
-    if (overload) atomicAdd(&overload[c], b);
+    atomicAdd(&ploss[uc], a);
+    if (overload) atomicAdd(&overload[uc], b);
   }
 }
 
@@ -1049,7 +1081,7 @@ __global__ void __launch_bounds__(256) k_adj_dldx(DevGrid d, int nbr, const doub
   load_outages(d, c, o);
   const int k1 = min(nbr, (int)(blockIdx.x + 1) * 64);
   for (int k = blockIdx.x * 64 + warp; k < k1; k += 8) {
-    if (outaged(o, k)) continue;
+    if (!branch_here(d, k, grp) || outaged(o, k)) continue;
     const int2 ft = d.br_ft[k];
     double2 y[4];
     branch_y(d, k, grp, lane, y);
@@ -1091,7 +1123,7 @@ __global__ void __launch_bounds__(128) k_mf_fsolve_t(DevLU L, const int* __restr
   for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
     const int s = task_sn[t / ngroups];
     const int g = (int)(t % ngroups);
-    if (!group_active[g]) continue;
+    if (!group_active[g] || !task_here(L, s, g)) continue;
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     for (int i = 0; i < f; ++i) b[i * 32 + lane] = (T)0;
@@ -1130,7 +1162,7 @@ __global__ void __launch_bounds__(128) k_mf_bsolve_t(DevLU L, const int* __restr
   for (long long t = (long long)blockIdx.x * warps + warp; t < ntasks; t += (long long)gridDim.x * warps) {
     const int s = task_sn[t / ngroups];
     const int g = (int)(t % ngroups);
-    if (!group_active[g]) continue;
+    if (!group_active[g] || !task_here(L, s, g)) continue;
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     const long long po = L.pan_off[s];
@@ -1154,9 +1186,10 @@ __global__ void k_adj_grad_bus(DevGrid d, int ncases, const T* __restrict__ lam,
                                double* __restrict__ gq) {
   const size_t total = (size_t)ncases * d.nb;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(t / d.nb), i = (int)(t % d.nb);
+    const int uc = (int)(t / d.nb), i = (int)(t % d.nb);
+    const int c = lane_of_case(d, uc);
     const int2 jv = d.jvar[i];
-    const bool ok = d.status[c] == ST_CONVERGED;
+    const bool ok = d.status[c] == ST_CONVERGED && row_here(d, i, c >> 5);
     if (gp) gp[t] = (ok && jv.x >= 0) ? (double)lam[at32(c >> 5, d.n_jac, jv.x, c & 31)] : 0.0;
     if (gq) gq[t] = (ok && jv.y >= 0) ? (double)lam[at32(c >> 5, d.n_jac, jv.y, c & 31)] : 0.0;
   }
@@ -1177,12 +1210,13 @@ __global__ void __launch_bounds__(256) k_adj_grad_branch(DevGrid d, int nbr, int
   const int c = grp * 32 + lane;
   LaneOut o;
   load_outages(d, c, o);
-  const bool ok = c < ncases && d.status[c] == ST_CONVERGED;
+  const int uc = case_of_lane(d, c, ncases);  // the user's case in this lane, -1 for padding
+  const bool ok = uc >= 0 && d.status[c] == ST_CONVERGED;
   const int k1 = min(nbr, (int)(blockIdx.x + 1) * 64);
   for (int k = blockIdx.x * 64 + warp; k < k1; k += 8) {
-    if (c >= ncases) continue;
+    if (uc < 0) continue;
     double rg = 0.0, rb = 0.0;
-    if (ok && !outaged(o, k)) {
+    if (ok && branch_here(d, k, grp) && !outaged(o, k)) {
       const int2 ft = d.br_ft[k];
       double2 y[4], a[4];
       branch_y(d, k, grp, lane, y);
@@ -1217,8 +1251,8 @@ __global__ void __launch_bounds__(256) k_adj_grad_branch(DevGrid d, int nbr, int
       rg -= lPf * Df.x + lQf * Df.y + lPt * Dt.x + lQt * Dt.y;
       rb -= lPf * Df.y - lQf * Df.x + lPt * Dt.y - lQt * Dt.x;
     }
-    if (gg) gg[(size_t)c * nbr + k] = rg;
-    if (gb) gb[(size_t)c * nbr + k] = rb;
+    if (gg) gg[(size_t)uc * nbr + k] = rg;
+    if (gb) gb[(size_t)uc * nbr + k] = rb;
   }
 }
 
@@ -1362,21 +1396,24 @@ __global__ void k_fill_int(int* p, int n, int v) {
 
 // ---------------------------------------------------------------- results
 // [group][bus][32] -> [case][bus]
-__global__ void k_gather_v(int nb, int ncases, const double2* V, double2* out) {
+// case_lane (nullable): lane of each case when lanes are grouped by island
+__global__ void k_gather_v(int nb, int ncases, const int* case_lane, const double2* V, double2* out) {
   const size_t total = (size_t)ncases * nb;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(t / nb), i = (int)(t % nb);
+    const int uc = (int)(t / nb), i = (int)(t % nb);
+    const int c = case_lane ? case_lane[uc] : uc;
     out[t] = V[at32(c >> 5, nb, i, c & 31)];
   }
 }
 
-__global__ void k_gather_small(int ncases, const int* status, const int* iters, const double* maxmis,
-                               uint8_t* st_out, int* it_out, double* mm_out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncases) return;
-  if (st_out) st_out[c] = (uint8_t)status[c];
-  if (it_out) it_out[c] = iters[c];
-  if (mm_out) mm_out[c] = maxmis[c];
+__global__ void k_gather_small(int ncases, const int* case_lane, const int* status, const int* iters,
+                               const double* maxmis, uint8_t* st_out, int* it_out, double* mm_out) {
+  const int uc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (uc >= ncases) return;
+  const int c = case_lane ? case_lane[uc] : uc;
+  if (st_out) st_out[uc] = (uint8_t)status[c];
+  if (it_out) it_out[uc] = iters[c];
+  if (mm_out) mm_out[uc] = maxmis[c];
 }
 
 }  // namespace mpfk

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <set>
 #include <string>
 #include <vector>
@@ -391,8 +392,8 @@ std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, i
       return "bus " + std::to_string(i) + " has a non-finite field";
     g.bus_type[i] = t;
     if (t == MPF_BUS_SLACK) {
-      if (g.slack >= 0) return "more than one slack bus";
-      g.slack = i;
+      if (g.slack < 0) g.slack = i;
+      ++g.n_slack;
     } else if (t == MPF_BUS_PV) {
       g.pv.push_back(i);
     } else if (t == MPF_BUS_PQ) {
@@ -412,6 +413,48 @@ std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, i
       return "branch " + std::to_string(e) + " has a non-finite field";
     if (b.x == 0.0) return "branch " + std::to_string(e) + " has zero reactance";
     if (b.status != 0 && b.status != 1) return "branch " + std::to_string(e) + " status must be 0 or 1";
+  }
+  // Islands: connected components over every branch (in or out of service).  Each
+  // component with PV/PQ buses needs exactly one slack; several islands make a
+  // multi-grid handle whose Jacobian is block-diagonal (one block per island).
+  {
+    std::vector<int> comp(nb);
+    for (int i = 0; i < nb; ++i) comp[i] = i;
+    std::function<int(int)> root = [&](int i) {
+      while (comp[i] != i) {
+        comp[i] = comp[comp[i]];
+        i = comp[i];
+      }
+      return i;
+    };
+    for (int e = 0; e < nbr; ++e) {
+      const int a = root(br[e].from), b = root(br[e].to);
+      if (a != b) comp[std::max(a, b)] = std::min(a, b);
+    }
+    std::vector<int> slack_of(nb, -1), free_of(nb, 0);
+    for (int i = 0; i < nb; ++i) {
+      const int r = root(i);
+      if (g.bus_type[i] == MPF_BUS_SLACK) {
+        if (slack_of[r] >= 0)
+          return "more than one slack bus in one connected island (buses " + std::to_string(slack_of[r]) + " and " +
+                 std::to_string(i) + ")";
+        slack_of[r] = i;
+      } else if (g.bus_type[i] == MPF_BUS_PV || g.bus_type[i] == MPF_BUS_PQ) {
+        ++free_of[r];
+      }
+    }
+    std::vector<int> island_of_root(nb, -1);
+    for (int i = 0; i < nb; ++i)  // islands numbered in the order of their slack buses
+      if (g.bus_type[i] == MPF_BUS_SLACK) island_of_root[root(i)] = g.n_islands++;
+    g.bus_island.assign(nb, -1);
+    for (int i = 0; i < nb; ++i) {
+      const int r = root(i);
+      if (free_of[r] > 0 && slack_of[r] < 0)
+        return "bus " + std::to_string(i) + " is in a connected island without a slack bus";
+      g.bus_island[i] = island_of_root[r];
+    }
+    g.br_island.resize(nbr);
+    for (int e = 0; e < nbr; ++e) g.br_island[e] = g.bus_island[br[e].from];
   }
   // Ybus superset pattern
   std::vector<std::vector<int>> rows(nb);

@@ -72,6 +72,8 @@ def n1_cases(branches, n_bus, n_out, seed, with_base=False):
 WORKLOADS = {
     "cfg0_30bus": dict(n_bus=30, n_branch=41, n_pv=5, tap_fraction=0.0, n_out=10, with_base=True),
     "cfg1_300bus": dict(n_bus=300, n_branch=411, n_pv=69, tap_fraction=0.10, n_out=200, with_base=False),
+    # 200 outages are asked for, but the 179-branch grid has 167 non-bridge branches:
+    # its N-1 set is all of them
     "cfg2_118bus": dict(n_bus=118, n_branch=179, n_pv=53, tap_fraction=0.10, n_out=200, with_base=False),
     "cfg2_1354bus": dict(n_bus=1354, n_branch=1991, n_pv=259, tap_fraction=0.10, n_out=400, with_base=False),
     "cfg2_2869bus": dict(n_bus=2869, n_branch=4582, n_pv=509, tap_fraction=0.10, n_out=400, with_base=False),
@@ -80,9 +82,27 @@ WORKLOADS = {
 }
 
 
+# Grids of uneven size solved as one batch (MultiGrid): config 2.
+WORKLOAD_SETS = {"cfg2": ["cfg2_118bus", "cfg2_1354bus", "cfg2_2869bus"]}
+
+
 def workload(name, seed=1, outage_seed=7):
-    """(buses, branches, cases) of a named workload."""
+    """(buses, branches, cases) of a named workload.  The N-1 set holds n_out
+    non-bridge outages, or every non-bridge branch when the grid has fewer."""
     w = WORKLOADS[name]
     buses, branches = synth_grid(w["n_bus"], w["n_branch"], w["n_pv"], w["tap_fraction"], seed=seed)
-    cases = n1_cases(branches, w["n_bus"], w["n_out"], outage_seed, w["with_base"]) if w["n_out"] else [[]]
+    n_out = w["n_out"]
+    if n_out:
+        n_out = min(n_out, int((find_bridges(branches, w["n_bus"]) == 0).sum()))
+    cases = n1_cases(branches, w["n_bus"], n_out, outage_seed, w["with_base"]) if n_out else [[]]
     return buses, branches, cases
+
+
+def workload_set(name, seed=1, outage_seed=7):
+    """(grids, cases_per_grid) of a named set of grids solved as one batch."""
+    grids, cases = [], []
+    for wname in WORKLOAD_SETS[name]:
+        b, br, cs = workload(wname, seed, outage_seed)
+        grids.append((b, br))
+        cases.append(cs)
+    return grids, cases

@@ -88,11 +88,18 @@ class PowerFlow:
             raise MpfError(rc, lib().mpf_last_error(self._h).decode())
 
     # -- cases and solves ----------------------------------------------------
-    def set_cases(self, cases, sbus=None):
-        """cases: list of outage lists (branch indices); sbus: (n_cases, n_bus, 2) or None."""
+    def set_cases(self, cases, sbus=None, islands=None):
+        """cases: list of outage lists (branch indices); sbus: (n_cases, n_bus, 2) or None;
+        islands (grids with several islands): the island of each case (mpf_set_cases_islands)."""
         offs, flat = cases_to_offsets(cases)
         sb = None if sbus is None else np.ascontiguousarray(sbus, dtype=np.float64)
-        self._check(lib().mpf_set_cases(self._h, len(cases), ptr(offs), ptr(flat), ptr(sb)))
+        if islands is None:
+            self._check(lib().mpf_set_cases(self._h, len(cases), ptr(offs), ptr(flat), ptr(sb)))
+        else:
+            isl = np.ascontiguousarray(islands, dtype=np.int32)
+            if isl.shape != (len(cases),):
+                raise ValueError("islands needs one entry per case")
+            self._check(lib().mpf_set_cases_islands(self._h, len(cases), ptr(isl), ptr(offs), ptr(flat), ptr(sb)))
         self.n_cases = len(cases)
 
     def set_controls(self, controls, values):
