@@ -385,6 +385,84 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def run_multigrid(args, rank, world, local_rank):
+    """Grids of uneven size in one batch (MultiGrid): every stage of the three grids'
+    cases runs in shared launches.  Beside it: the same cases on one handle per grid,
+    solved back to back on the same stream."""
+    import torch
+
+    import mapol_b200 as m
+    from mapol_b200 import _types as T
+    from mapol_b200.grid import WORKLOAD_SETS, workload_set
+    from mapol_b200.shard import max_over_ranks as _mor
+
+    torch.cuda.set_device(local_rank)
+    grids, cases = workload_set(args.workload)
+    n_cases = sum(len(c) for c in cases)
+    stream = torch.cuda.current_stream()
+
+    def timed(solve_all):
+        for _ in range(args.warmup):
+            solve_all()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            solve_all()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return _mor(e0.elapsed_time(e1), world, "cuda")
+
+    out = {}
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    with m.MultiGrid(grids, device=local_rank) as mg:
+        mg.set_cases(cases)
+        for prec, name in ((m.MIXED, "mixed"), (m.FP64, "fp64")):
+            ms = timed(lambda: mg.pf.solve(m.NR, prec, stream.cuda_stream))
+            res = mg.results()
+            out[name] = dict(ms=ms, launches=mg.timing()["launches"],
+                             n_conv=int(sum((r.status == T.CASE_CONVERGED).sum() for r in res)))
+    pfs = []
+    for (b, br), cs in zip(grids, cases):
+        pf = m.PowerFlow(b, br, device=local_rank)
+        pf.set_cases(cs)
+        pfs.append(pf)
+
+    def separate():
+        for pf in pfs:
+            pf.solve(m.NR, m.MIXED, stream.cuda_stream)
+
+    sep_ms = timed(separate)
+    sep_launches = sum(pf.timing()["launches"] for pf in pfs)
+    for pf in pfs:
+        pf.close()
+    clocks = sampler.stop() if sampler else None
+    if rank != 0:
+        return None
+    value = n_cases * world * args.steps / (out["mixed"]["ms"] / 1e3)
+    return {
+        "metric": "PF solves/sec @1e-8 pu, grids of uneven size in one batch (%s-bus synth): mixed vs plain FP64"
+                  % "/".join(str(len(g[0])) for g in grids),
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": out["mixed"]["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 mismatch/update/convergence test, f32 LU factorisation and solves",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": args.workload, "grids": WORKLOAD_SETS[args.workload],
+                   "cases_per_grid": [len(c) for c in cases], "alg": "NR"},
+        "plain_fp64": {"value": n_cases * world * args.steps / (out["fp64"]["ms"] / 1e3),
+                       "ms_per_step": out["fp64"]["ms"] / args.steps},
+        "converged": {"mixed": out["mixed"]["n_conv"], "fp64": out["fp64"]["n_conv"], "of": n_cases},
+        "launches_per_solve": {"one_batch": out["mixed"]["launches"], "one_handle_per_grid": sep_launches},
+        "one_handle_per_grid": {"value": n_cases * world * args.steps / (sep_ms / 1e3),
+                                "ms_per_step": sep_ms / args.steps, "precision": "mixed"},
+        "clocks": clocks,
+    }
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -404,7 +482,12 @@ def main():
 
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    line = run_ours(args, rank, world, local_rank)
+    from mapol_b200.grid import WORKLOAD_SETS
+
+    if args.workload in WORKLOAD_SETS:
+        line = run_multigrid(args, rank, world, local_rank)
+    else:
+        line = run_ours(args, rank, world, local_rank)
     if world > 1:
         import torch
 
