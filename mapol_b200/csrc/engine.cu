@@ -17,6 +17,7 @@
 #include <mutex>
 #include <set>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -90,6 +91,25 @@ struct Launch {
   int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
 };
 
+// FNV-1a over the structure that decides the launches and their work
+inline uint64_t structure_fingerprint(const LUSymbolic& s) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](int64_t v) {
+    for (int b = 0; b < 8; ++b) {
+      h ^= (uint64_t)((v >> (8 * b)) & 0xff);
+      h *= 1099511628211ull;
+    }
+  };
+  mix(s.n);
+  mix(s.nnz);
+  mix(s.nsn);
+  for (int v : s.sn_w) mix(v);
+  for (int v : s.sn_f) mix(v);
+  for (int v : s.lev_ptr) mix(v);
+  for (int v : s.lev_sn) mix(v);
+  return h;
+}
+
 // Kernel of one factorisation launch: kind 0 = warp teams (k_mf_factor<T, ge, 32>,
 // tpb teams per block), 1 = 256-thread teams with the LU in shared memory, 2 = the
 // same with the LU in registers (TT x TT tile per thread)
@@ -105,7 +125,10 @@ struct LUSystem {
   const int* group_island = nullptr; // the handle's current per-group islands (or null)
   std::vector<Launch> factor_sched;  // ascending levels
   // autotuned kernel of every factor_sched launch, per (precision, case groups)
+  uint64_t fingerprint = 0;          // of the symbolic structure (process-wide tuning cache key)
   std::map<std::pair<int, int>, std::vector<FactorChoice>> tuned;
+  // autotuned lane count of every backward-solve level launch (0 = one case per thread)
+  std::map<std::pair<int, int>, std::vector<int>> tuned_bs;
   std::vector<Launch> level_sched;   // one launch per level (solves), ascending
   int nA = 0;
   // values per precision [0] = FP64, [1] = FP32
@@ -171,6 +194,7 @@ struct LUSystem {
     upload(cb_off, co);
     upload(cbr_off, ro);
     upload(lev_sn, s.lev_sn);
+    fingerprint = structure_fingerprint(s);
     factor_sched.clear();
     level_sched.clear();
     for (int l = 0; l < s.nlevels; ++l) {
@@ -257,6 +281,7 @@ void ensure_attrs(int device) {
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 32, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G / 2, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 8, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
@@ -408,6 +433,10 @@ std::vector<FactorChoice> factor_candidates(const Launch& ln, int ngroups) {
   }
   for (int tpb : {8, 4, 2})
     if (factor_smem_rt(ln.fcap, G, tpb, 0, ws) <= kSmemMax) add({0, G, 0, tpb});
+  // half-width lane chunks: half the shared memory per warp, twice the resident warps
+  if (ln.fcap <= kFmaxM)
+    for (int tpb : {8, 4})
+      if (factor_smem_rt(ln.fcap, G / 2, tpb, 0, ws) <= kSmemMax) add({0, G / 2, 0, tpb});
   for (int ge = G; ge >= 1; ge /= 2)
     if (factor_smem_rt(ln.fcap, ge, 1, 0, ws) <= kSmemMax) add({1, ge, 0, 1});
   const int tt = reg_tt(ln.fcap);
@@ -424,8 +453,13 @@ void launch_choice(const FactorChoice& ch, const LUSystem& sys, const Launch& ln
   if (ch.kind == 0) {
     if (ch.ge == 32)
       launch_factor_one<T, 32, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, ch.tpb);
-    else
+    else if (ch.ge == G)
       launch_factor_one<T, G, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, ch.tpb);
+    else if (ch.ge == G / 2)
+      launch_factor_one<T, G / 2, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st,
+                                      ch.tpb);
+    else
+      throw MpfError{MPF_ERR_INTERNAL, "no warp-team kernel for this lane count"};
   } else if (ch.kind == 1) {
     if (ch.ge == 32)
       launch_factor_one<T, 32, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
@@ -454,10 +488,33 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
 // (CUDA events).  Runs without the right-hand side, so x is not touched; every
 // candidate computes the same panels and contribution blocks, which the next
 // level reads.  Called outside stream capture, once per (precision, groups).
+// Process-wide tuning results, keyed by (structure fingerprint, precision, groups): every
+// handle of the same grid and batch size in a process runs the same kernels, so their
+// results agree bit for bit (kernels that split a dot product differently round
+// differently).
+struct TuneCache {
+  std::mutex mu;
+  std::map<std::tuple<uint64_t, int, int>, std::vector<FactorChoice>> factor;
+  std::map<std::tuple<uint64_t, int, int>, std::vector<int>> bsolve;
+};
+inline TuneCache& tune_cache() {
+  static TuneCache c;
+  return c;
+}
+
 template <typename T>
 void tune_factor(LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x, int* status,
                  const int* group_active, cudaStream_t st) {
   if (sys.tuned.count({Prec<T>::idx, ngroups})) return;
+  const auto key = std::make_tuple(sys.fingerprint, Prec<T>::idx, ngroups);
+  {
+    std::lock_guard<std::mutex> lock(tune_cache().mu);
+    const auto it = tune_cache().factor.find(key);
+    if (it != tune_cache().factor.end()) {
+      sys.tuned[{Prec<T>::idx, ngroups}] = it->second;
+      return;
+    }
+  }
   cudaEvent_t e0, e1;
   CUDA_TRY(cudaEventCreate(&e0));
   CUDA_TRY(cudaEventCreate(&e1));
@@ -506,41 +563,119 @@ void tune_factor(LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, 
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   sys.tuned[{Prec<T>::idx, ngroups}] = best;
+  std::lock_guard<std::mutex> lock(tune_cache().mu);
+  tune_cache().factor.emplace(key, best);
+}
+
+// Backward substitution of one level: ge = 0 one case per thread (k_mf_bsolve), else
+// warps over chunks of ge lanes (k_mf_bsolve_chunk).
+template <typename T>
+void launch_bsolve_one(int ge, const LUSystem& sys, const Launch& ln, int ngroups, const T* pan, T* x,
+                       const int* group_active, cudaStream_t st) {
+  const DevLU dl = sys.dev();
+  const int* ts = sys.lev_sn.as<int>() + ln.offset;
+  const long long ntasks = (long long)ln.count * ngroups * (ge ? 32 / ge : 1);
+  const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
+  const size_t smem = (size_t)4 * ln.fcap * (ge ? ge : 32) * sizeof(T);
+  switch (ge) {
+    case 0: k_mf_bsolve<T><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 8: k_mf_bsolve_chunk<T, 8><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 4: k_mf_bsolve_chunk<T, 4><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 2: k_mf_bsolve_chunk<T, 2><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 1: k_mf_bsolve_chunk<T, 1><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    default: throw MpfError{MPF_ERR_INTERNAL, "no backward-solve kernel for this lane count"};
+  }
+  CUDA_TRY(cudaGetLastError());
+}
+
+// the fixed rule: one case per thread for small fronts; on levels with few
+// supernodes, fewer lanes per warp (more warps, more slots per lane)
+template <typename T>
+int bsolve_heuristic(const Launch& ln, int ngroups) {
+  if (ln.fcap <= kFmaxM1) return 0;
+  int ge = Prec<T>::G;
+  while (ge > 1 && (long long)ln.count * ngroups * (32 / ge) < 148LL * 16) ge /= 2;
+  return ge;
 }
 
 template <typename T>
 void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active, cudaStream_t st,
                    int* nlaunch) {
-  constexpr int G = Prec<T>::G;
+  const auto it = sys.tuned_bs.find({Prec<T>::idx, ngroups});
   for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
     const Launch& ln = sys.level_sched[k];
-    if (ln.fcap <= kFmaxM1) {
-      // small fronts: one case per thread
-      const long long ntasks = (long long)ln.count * ngroups;
-      const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-      const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
-      k_mf_bsolve<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
-                                                          ngroups, ln.fcap, pan, x, group_active);
-    } else {
-      // chunked: fewer lanes per warp (more warps, more slots per lane) on levels
-      // with few supernodes
-      int ge = G;
-      while (ge > 1 && (long long)ln.count * ngroups * (32 / ge) < 148LL * 16) ge /= 2;
-      const long long ntasks = (long long)ln.count * ngroups * (32 / ge);
-      const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-      const size_t smem = (size_t)4 * ln.fcap * ge * sizeof(T);
-      const DevLU dl = sys.dev();
-      const int* ts = sys.lev_sn.as<int>() + ln.offset;
-      switch (ge) {
-        case 8: k_mf_bsolve_chunk<T, 8><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-        case 4: k_mf_bsolve_chunk<T, 4><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-        case 2: k_mf_bsolve_chunk<T, 2><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-        default: k_mf_bsolve_chunk<T, 1><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-      }
-    }
-    CUDA_TRY(cudaGetLastError());
+    const int ge = it != sys.tuned_bs.end() ? it->second[k] : bsolve_heuristic<T>(ln, ngroups);
+    launch_bsolve_one<T>(ge, sys, ln, ngroups, pan, x, group_active, st);
     ++*nlaunch;
   }
+}
+
+// Autotuner of the backward solve: per level, each lane count runs twice and the
+// faster second run is kept.  The runs overwrite x, whose values do not change the
+// timing; x is saved first and restored after.  Outside stream capture, once per
+// (precision, groups).
+template <typename T>
+void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active, cudaStream_t st) {
+  if (sys.tuned_bs.count({Prec<T>::idx, ngroups})) return;
+  const auto key = std::make_tuple(sys.fingerprint, Prec<T>::idx, ngroups);
+  {
+    std::lock_guard<std::mutex> lock(tune_cache().mu);
+    const auto it = tune_cache().bsolve.find(key);
+    if (it != tune_cache().bsolve.end()) {
+      sys.tuned_bs[{Prec<T>::idx, ngroups}] = it->second;
+      return;
+    }
+  }
+  const size_t xbytes = (size_t)ngroups * 32 * sys.sym.n * sizeof(T);
+  DevBuf saved;
+  saved.alloc(xbytes);
+  CUDA_TRY(cudaMemcpyAsync(saved.p, x, xbytes, cudaMemcpyDeviceToDevice, st));
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  std::vector<int> best(sys.level_sched.size(), 0);
+  const bool log = std::getenv("MPF_TUNE_LOG") != nullptr;
+  double sum_best = 0.0, sum_heur = 0.0;
+  try {
+    for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
+      const Launch& ln = sys.level_sched[k];
+      const int h0 = bsolve_heuristic<T>(ln, ngroups);
+      std::vector<int> cands{h0};
+      for (int ge : {0, 8, 4, 2, 1})
+        if (ge != h0) cands.push_back(ge);
+      float bt = 0.0f, ht = 0.0f;
+      for (size_t i = 0; i < cands.size(); ++i) {
+        launch_bsolve_one<T>(cands[i], sys, ln, ngroups, pan, x, group_active, st);
+        CUDA_TRY(cudaEventRecord(e0, st));
+        launch_bsolve_one<T>(cands[i], sys, ln, ngroups, pan, x, group_active, st);
+        CUDA_TRY(cudaEventRecord(e1, st));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (i == 0) ht = ms;
+        if (i == 0 || ms < bt) {
+          bt = ms;
+          best[k] = cands[i];
+        }
+      }
+      sum_best += bt;
+      sum_heur += ht;
+    }
+    if (log)
+      std::fprintf(stderr, "mpf tune: n %d fp%d groups %d backward solve heuristic %.3f ms, tuned %.3f ms\n",
+                   sys.sym.n, (int)sizeof(T) * 8, ngroups, sum_heur, sum_best);
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CUDA_TRY(cudaMemcpyAsync(x, saved.p, xbytes, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  sys.tuned_bs[{Prec<T>::idx, ngroups}] = best;
+  std::lock_guard<std::mutex> lock(tune_cache().mu);
+  tune_cache().bsolve.emplace(key, best);
 }
 
 template <typename T>
@@ -915,8 +1050,10 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
   int it = 0;
   // pick the factorisation kernels of this batch size (first solve only), before
   // the iteration is captured
-  if (h->opt.autotune && max_it > 0 && any_active(h, st))
+  if (h->opt.autotune && max_it > 0 && any_active(h, st)) {
     tune_factor<T>(J, h->ngroups, A, pan, cb, cbr, x, d.status, d.group_active, st);
+    tune_bsolve<T>(J, h->ngroups, pan, x, d.group_active, st);
+  }
   auto& gph = h->nr_graph[P];
   if (h->opt.use_graph) {
     // the captured kernels hold every device pointer of d by value: capture again
@@ -1017,6 +1154,11 @@ void solve_fd(mpf_handle* h, cudaStream_t st, int variant) {
                      S.x[P].as<T>(), d.status, d.group_active, 0, st, &nl);
   }
   tm.end(ev);
+  if (h->opt.autotune)
+    for (int k = 0; k < 2; ++k) {
+      LUSystem& S = *systems[k];
+      tune_bsolve<T>(S, h->ngroups, S.pan[P].as<T>(), S.x[P].as<T>(), d.group_active, st);
+    }
   T* xp = Bp.x[P].as<T>();
   T* xq = Bpp.x[P].as<T>();
   const int max_it = h->opt.max_it_fd;
