@@ -9,7 +9,8 @@ import os
 from . import _types as T
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libmpf.so")
+# MPF_LIB_PATH: load another build of the same library (e.g. to compare two builds)
+LIB_PATH = os.environ.get("MPF_LIB_PATH") or os.path.join(_HERE, "libmpf.so")
 
 _lib = None
 

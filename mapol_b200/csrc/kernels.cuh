@@ -285,6 +285,25 @@ constexpr int kRowsPerBlock = 64;
 //   V_i = a + jb, V_j = c + jd, yv = Y_ij V_j, w = yv / |V_j|, I = Ibus_i if i == j else 0
 //   dP/dVa = -b (I_r - yv_r) - a (-I_i + yv_i)     dP/dVm = a w_r + b w_i + (I_r c + I_i d)/|V_j|
 //   dQ/dVa = -b (-I_i + yv_i) + a (I_r - yv_r)     dQ/dVm = -a w_i + b w_r + (I_r d - I_i c)/|V_j|
+// J entries of Ybus entry (i, j) of this lane's case, written at the arrowhead
+// positions jp (-1: not a J entry).  I = Ibus_i on the diagonal, 0 elsewhere.
+template <typename T>
+__device__ __forceinline__ void jac_entry(const DevGrid& d, T* A, int g, int lane, int4 jp, double2 y, double2 vj,
+                                          double a, double b, double ir, double ii) {
+  const double cc = vj.x, dd = vj.y;
+  const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
+  if (jp.x >= 0) A[at32(g, d.nA_jac, jp.x, lane)] = (T)(-b * (ir - yvr) - a * (-ii + yvi));
+  if (jp.z >= 0) A[at32(g, d.nA_jac, jp.z, lane)] = (T)(-b * (-ii + yvi) + a * (ir - yvr));
+  if (jp.y >= 0 || jp.w >= 0) {
+    const double inv = 1.0 / sqrt(cc * cc + dd * dd);  // 1 / |V_j|
+    const double wr = yvr * inv, wi = yvi * inv;
+    if (jp.y >= 0) A[at32(g, d.nA_jac, jp.y, lane)] = (T)(a * wr + b * wi + (ir * cc + ii * dd) * inv);
+    if (jp.w >= 0) A[at32(g, d.nA_jac, jp.w, lane)] = (T)(-a * wi + b * wr + (ir * dd - ii * cc) * inv);
+  }
+}
+
+// One pass over the row: the off-diagonal J entries need no Ibus and are written
+// while Ibus accumulates; the diagonal entry follows once Ibus is complete.
 template <typename T, bool JAC, bool CTL>
 __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
   const int g = blockIdx.y;
@@ -301,13 +320,18 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
     double2 ib = make_double2(0.0, 0.0);
     const int p0 = d.y_rowptr[i], p1 = d.y_rowptr[i + 1];
     const bool touched = row_touched(o, d.y_diag[i]);
+    const double2 vi = d.V[at32(g, d.nb, i, lane)];
     for (int p = p0; p < p1; ++p) {
+      const int j = d.y_col[p];
       const double2 y = yentry<CTL>(d, o, touched, p, g, lane);
-      const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
+      const double2 v = j == i ? vi : d.V[at32(g, d.nb, j, lane)];
       ib.x += y.x * v.x - y.y * v.y;
       ib.y += y.x * v.y + y.y * v.x;
+      if (JAC && j != i) {
+        const int4 jp = d.jpos[p];
+        if (jp.x >= 0 || jp.y >= 0 || jp.z >= 0 || jp.w >= 0) jac_entry<T>(d, A, g, lane, jp, y, v, vi.x, vi.y, 0.0, 0.0);
+      }
     }
-    const double2 vi = d.V[at32(g, d.nb, i, lane)];
     const double2 s = d.sbus_case ? d.sbus_case[at32(g, d.nb, i, lane)] : d.sbus0[i];
     // mis = V conj(Ibus) - S
     const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
@@ -323,25 +347,9 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
     if (mr != mr) m = INFINITY;
     lmax = fmax(lmax, finite_or_inf(m));
     if (JAC) {
-      const double a = vi.x, b = vi.y;
-      for (int p = p0; p < p1; ++p) {
-        const int4 jp = d.jpos[p];
-        if (jp.x < 0 && jp.y < 0 && jp.z < 0 && jp.w < 0) continue;
-        const int j = d.y_col[p];
-        const double2 y = yentry<CTL>(d, o, touched, p, g, lane);
-        const double2 vj = d.V[at32(g, d.nb, j, lane)];
-        const double cc = vj.x, dd = vj.y;
-        const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
-        const double ir = (i == j) ? ib.x : 0.0, ii = (i == j) ? ib.y : 0.0;
-        if (jp.x >= 0) A[at32(g, d.nA_jac, jp.x, lane)] = (T)(-b * (ir - yvr) - a * (-ii + yvi));
-        if (jp.z >= 0) A[at32(g, d.nA_jac, jp.z, lane)] = (T)(-b * (-ii + yvi) + a * (ir - yvr));
-        if (jp.y >= 0 || jp.w >= 0) {
-          const double ab = sqrt(cc * cc + dd * dd);
-          const double wr = yvr / ab, wi = yvi / ab;
-          if (jp.y >= 0) A[at32(g, d.nA_jac, jp.y, lane)] = (T)(a * wr + b * wi + (ir * cc + ii * dd) / ab);
-          if (jp.w >= 0) A[at32(g, d.nA_jac, jp.w, lane)] = (T)(-a * wi + b * wr + (ir * dd - ii * cc) / ab);
-        }
-      }
+      const int pd = d.y_diag[i];
+      const int4 jp = d.jpos[pd];
+      jac_entry<T>(d, A, g, lane, jp, yentry<CTL>(d, o, touched, pd, g, lane), vi, vi.x, vi.y, ib.x, ib.y);
     } else {
       d.Ibus[at32(g, d.nb, i, lane)] = ib;
     }

@@ -169,8 +169,10 @@ def test_full_size_9241_bus_sample_matches_oracle(gpu):
 
 
 def test_mismatch_entry_point_matches_solve_and_oracle(gpu):
-    """mpf_mismatch at the solved voltages reproduces the solve's own final max |F|
-    and the oracle's mismatch at the same voltages."""
+    """mpf_mismatch at the solved voltages reproduces the solve's own final max |F| (both
+    round-off there, so to 1e-13 absolute: the solve's fused mismatch-Jacobian pass and
+    this evaluation kernel order their operations differently) and, at an unconverged
+    point, the oracle's mismatch to 1e-12 relative."""
     import torch
 
     from mapol_b200._lib import lib
@@ -187,7 +189,8 @@ def test_mismatch_entry_point_matches_solve_and_oracle(gpu):
             assert lib().mpf_mismatch(pf._h, v.data_ptr(), out.data_ptr(), None) == 0
             torch.cuda.synchronize()
             got = out.cpu().numpy()
-            np.testing.assert_allclose(got, res.max_mis, rtol=1e-6, atol=1e-15)
+            np.testing.assert_allclose(got, res.max_mis, rtol=1e-6, atol=1e-13)
+            assert (got < 1e-8).all()
         # an unconverged point: the flat start
         flat = np.zeros((len(cases), len(buses)), complex)
         flat[:] = buses["vm"] * np.exp(1j * buses["va"])
