@@ -677,8 +677,21 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : 4) k_mf_
     team_sync<TEAM>();
     {
       const T* a0 = A + at32(g, L.nA, 0, lane);
-      for (int e = L.ah_ptr[s] + slot; e < L.ah_ptr[s + 1]; e += SLOTS)
-        st<T, V>(F + L.ah_loc[e] * G, ld<T, V>(a0 + (size_t)e * 32));
+      // four entries' index and value loads in flight before their stores
+      const int e1 = L.ah_ptr[s + 1];
+      int e = L.ah_ptr[s] + slot;
+      for (; e + 3 * SLOTS < e1; e += 4 * SLOTS) {
+        int loc[4];
+        LV v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          loc[u] = L.ah_loc[e + u * SLOTS];
+          v[u] = ld<T, V>(a0 + (size_t)(e + u * SLOTS) * 32);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) st<T, V>(F + loc[u] * G, v[u]);
+      }
+      for (; e < e1; e += SLOTS) st<T, V>(F + L.ah_loc[e] * G, ld<T, V>(a0 + (size_t)e * 32));
     }
     if (with_rhs)
       for (int p = slot; p < w; p += SLOTS) st<T, V>(FP(p, f), ld<T, V>(x + at32(g, L.n, rows[p], lane)));
@@ -813,6 +826,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : 4) k_mf_
       for (int p = rs; p < w; p += RSL) {
         T* dst = pbase + (size_t)p * f * 32;
         const T* src = FP(p, 0);
+#pragma unroll 4
         for (int q = c0; q < c1; ++q) st<T, V>(dst + (size_t)q * 32, ld<T, V>(src + q * G));
       }
     }
@@ -822,6 +836,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : 4) k_mf_
       for (int i = rs; i < m; i += RSL) {
         T* dst = pbase + ((size_t)w * f + (size_t)i * w) * 32;
         const T* src = FP(w + i, 0);
+#pragma unroll 4
         for (int q = c0; q < c1; ++q) st<T, V>(dst + (size_t)q * 32, ld<T, V>(src + q * G));
       }
     }
@@ -833,6 +848,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : 4) k_mf_
       for (int a = rs; a < m; a += RSL) {
         T* dst = cbase + (size_t)a * m * 32;
         const T* src = FP(w + a, w);
+#pragma unroll 4
         for (int b = c0; b < c1; ++b) st<T, V>(dst + (size_t)b * 32, ld<T, V>(src + b * G));
         if (with_rhs && cg == 0) st<T, V>(cbr + at32(g, L.sumcbr, L.cbr_off[s] + a, lane), ld<T, V>(FP(w + a, f)));
       }
