@@ -369,7 +369,7 @@ def run_ours(args, rank, world, local_rank):
         "mixed": {"converged": mixed["n_conv"], "iterations_hist": mixed["iters"], "max_mismatch": mixed["max_mis"]},
         "roofline": {"bound": "hbm", "kernel": dom.replace("_ms", ""), "achieved": round(achieved, 1),
                      "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "traffic_unit": "DRAM bytes per factorisation of all cases (its 45 launches)",
+                     "traffic_unit": "DRAM bytes per factorisation of all cases (all its level launches)",
                      "alg_bytes": alg_bytes("factor_ms", 4) * n_cases,
                      "traffic_source": "ncu dram__bytes_read+write.sum, 256 cases, per case x cases "
                                        "(profiles/dram_nr_mixed_9241bus_256cases.md)",
