@@ -184,6 +184,25 @@ int32_t mpf_set_cases_islands(mpf_handle* h, int32_t n_cases, const int32_t* isl
                               const int32_t* outage_offsets, const int32_t* outage_branches,
                               const double* sbus);
 
+/* Reactive-power limits of PV buses (PV -> PQ switching).  No counterpart in the
+ * reference, which parses generator Q limits (src/files/loadMatpowerFormat.h:130-137)
+ * and never enforces them.  qmin / qmax: per bus, limits of the net reactive injection
+ * in p.u. (generators' Qmin / Qmax minus the reactive load); +-inf or NaN = no limit;
+ * only PV buses with a finite limit are affected; NULL for both disables the limits.
+ * The Newton system gets a Vm variable and a Q equation for every limited PV bus (one
+ * pattern for all cases; while a bus is PV in a case its Q equation reads dVm = 0).
+ * mpf_solve(MPF_NR) then runs Newton to convergence, switches every PV bus whose Q lies
+ * outside its limits to PQ with Q held at the violated limit (all violators of a case
+ * at once, as MATPOWER's runpf with ENFORCE_Q_LIMS = 1), solves those cases again from
+ * their voltages, and repeats until no case has a new violation (at most 20 rounds);
+ * iteration counts add up over the rounds.  Fast-decoupled solves are refused while
+ * limits are set.  Rebuilds the Newton system: call before mpf_set_cases, which must
+ * be called again afterwards. */
+int32_t mpf_set_q_limits(mpf_handle* h, const double* qmin, const double* qmax);
+/* Bus types after the last solve, [n_cases][n_bus] (host): the grid's types, with the
+ * PV buses a case switched to PQ reading MPF_BUS_PQ. */
+int32_t mpf_get_bus_types(mpf_handle* h, uint8_t* types);
+
 /* Per-case control overrides: the optimiser's structures of
  * src/pso/Particula.h:26-60 (kinds keep the values of its enum Tipo), applied as
  * hybrid_computeVoltage (src/powerflow/runpf.h:524-541) and hybrid_computeYfYt

@@ -30,6 +30,8 @@ _SIGNATURES = {
     "mpf_set_cases": (c_i32, [c_p, c_i32, c_p, c_p, c_p]),
     "mpf_set_controls": (c_i32, [c_p, c_i32, c_p, c_p]),
     "mpf_set_cases_islands": (c_i32, [c_p, c_i32, c_p, c_p, c_p, c_p]),
+    "mpf_set_q_limits": (c_i32, [c_p, c_p, c_p]),
+    "mpf_get_bus_types": (c_i32, [c_p, c_p]),
     "mpf_solve": (c_i32, [c_p, c_i32, c_i32, c_p]),
     "mpf_get_results": (c_i32, [c_p, c_p, c_p, c_p, c_p]),
     "mpf_get_results_device": (c_i32, [c_p, c_p, c_p, c_p, c_p, c_p]),

@@ -84,6 +84,8 @@ enum TaskClass { CLS_S = 0, CLS_M = 1, CLS_L = 2, CLS_M1 = 3 };
 // 32-byte chunk would not fit in shared memory (kSmemMax)
 constexpr int kFmaxS = 8, kFmaxM1 = 16, kFmaxM = 24;
 constexpr size_t kSmemMax = 227 * 1024;
+// rounds of PV -> PQ switching per solve (each switches at least one bus of a case)
+constexpr int kMaxQRounds = 20;
 // largest front any task class can hold: one FP64 lane, f * ((f + 1) | 1) * 8 bytes
 constexpr int kFmaxAll = 167;
 
@@ -760,6 +762,11 @@ struct mpf_handle {
   // batch the island of each group and the case <-> lane maps
   DevBuf bus_island, br_island, group_island, lane_case, case_lane;
   std::vector<int> h_lane_case;
+  // reactive limits: PV buses with limits (a Vm variable each), their limits, and per
+  // batch the PV / switched state of each case
+  int nsw = 0;
+  std::vector<char> vm_free;         // per bus: PV bus with limits
+  DevBuf sw_index, sw_bus, q_lim, base_type, pv_on, q_fix, q_flag, iter_base;
   std::vector<mpf_bus> buses;        // the grid as given (controls read base values)
   std::vector<mpf_branch> branches;
   // per-case controls of the current cases (mpf_set_controls)
@@ -839,6 +846,13 @@ struct mpf_handle {
       d.lane_case = lane_case.as<int>();
       d.case_lane = case_lane.as<int>();
     }
+    if (nsw > 0 && pv_on.p) {
+      d.nsw = nsw;
+      d.sw_index = sw_index.as<int>();
+      d.pv_on = pv_on.as<unsigned char>();
+      d.q_fix = q_fix.as<double>();
+      d.iter_base = iter_base.as<int>();
+    }
     if (ctl.nc > 0) {
       d.nslot = ctl.nslot;
       d.noltc = ctl.noltc;
@@ -879,7 +893,8 @@ struct mpf_handle {
     const DevBuf* all[] = {&y_rowptr, &y_col, &y_val, &y_diag, &br_ft, &rating, &br_ypos, &br_y, &sbus0, &v0, &mis_rows, &jvar, &jpos,
                            &out_br, &sbus_case, &V, &Ibus, &status, &iters, &maxmis, &facc, &group_active,
                            &any_active, &vout, &small_out, &fdvar, &eval_acc, &it_ctr, &br_dy,
-                           &adj_status, &bus_island, &br_island, &group_island, &lane_case, &case_lane};
+                           &adj_status, &bus_island, &br_island, &group_island, &lane_case, &case_lane,
+                           &sw_index, &sw_bus, &q_lim, &base_type, &pv_on, &q_fix, &q_flag, &iter_base};
     for (auto p : all) b += p->bytes;
     b += ctl.bytes();
     const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
@@ -897,6 +912,28 @@ struct mpf_handle {
 };
 
 namespace {
+
+// The Newton system's device arrays: variable map, Jacobian positions, the LU system.
+void upload_newton(mpf_handle* h) {
+  const GridSymbolic& g = h->g;
+  std::vector<int2> jv(g.nb);
+  for (int i = 0; i < g.nb; ++i) jv[i] = make_int2(g.var_va[i], g.var_vm[i]);
+  upload(h->jvar, jv);
+  std::vector<int4> jp(g.y_col.size());
+  for (size_t p = 0; p < jp.size(); ++p)
+    jp[p] = make_int4(g.jpos[4 * p], g.jpos[4 * p + 1], g.jpos[4 * p + 2], g.jpos[4 * p + 3]);
+  upload(h->jpos, jp);
+  if (g.n_islands > 1) {
+    std::vector<int> vi(g.jac.n, -1);
+    for (int i = 0; i < g.nb; ++i) {
+      if (g.var_va[i] >= 0) vi[g.var_va[i]] = g.bus_island[i];
+      if (g.var_vm[i] >= 0) vi[g.var_vm[i]] = g.bus_island[i];
+    }
+    h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac, &vi);
+  } else {
+    h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac);
+  }
+}
 
 int fail(mpf_handle* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -959,16 +996,22 @@ bool any_active(mpf_handle* h, cudaStream_t st) {
   return *h->h_any != 0;
 }
 
+template <typename T, bool QL>
+void launch_mismatch_nr_q(const DevGrid& d, dim3 rg, cudaStream_t st, T* x, T* A, bool jac) {
+  const bool ctl = d.y_slot != nullptr;
+  if (jac && ctl) k_mismatch_nr<T, true, true, QL><<<rg, 256, 0, st>>>(d, x, A);
+  else if (jac) k_mismatch_nr<T, true, false, QL><<<rg, 256, 0, st>>>(d, x, A);
+  else if (ctl) k_mismatch_nr<T, false, true, QL><<<rg, 256, 0, st>>>(d, x, A);
+  else k_mismatch_nr<T, false, false, QL><<<rg, 256, 0, st>>>(d, x, A);
+  CUDA_TRY(cudaGetLastError());
+}
+
 // Newton mismatch (with the Jacobian when jac), in its variant with or without
-// per-case Ybus controls
+// per-case Ybus controls and reactive limits
 template <typename T>
 void launch_mismatch_nr(const DevGrid& d, dim3 rg, cudaStream_t st, T* x, T* A, bool jac) {
-  const bool ctl = d.y_slot != nullptr;
-  if (jac && ctl) k_mismatch_nr<T, true, true><<<rg, 256, 0, st>>>(d, x, A);
-  else if (jac) k_mismatch_nr<T, true, false><<<rg, 256, 0, st>>>(d, x, A);
-  else if (ctl) k_mismatch_nr<T, false, true><<<rg, 256, 0, st>>>(d, x, A);
-  else k_mismatch_nr<T, false, false><<<rg, 256, 0, st>>>(d, x, A);
-  CUDA_TRY(cudaGetLastError());
+  if (d.sw_index) launch_mismatch_nr_q<T, true>(d, rg, st, x, A, jac);
+  else launch_mismatch_nr_q<T, false>(d, rg, st, x, A, jac);
 }
 
 // AVR controls: the set-points of the current cases into V (after k_init)
@@ -1037,8 +1080,21 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
   CUDA_TRY(cudaGetLastError());
   ++nl;
   nl += apply_avr(h, st);
+  if (h->nsw > 0) {
+    const size_t tot = (size_t)h->ngroups * 32 * h->nsw;
+    k_qlim_reset<<<(unsigned)std::min<size_t>(148 * 8, tot / 256 + 1), 256, 0, st>>>(d);
+    CUDA_TRY(cudaGetLastError());
+    ++nl;
+  }
   tm.end(ev);
   const int max_it = h->opt.max_it_nr;
+  static const int kFam[4] = {FAM_FACT, FAM_SOLVE, FAM_UPD, FAM_MIS};
+  int it_total = 0;
+  auto& gph = h->nr_graph[P];
+  // one Newton run over the running cases: mismatch at the current voltages, check,
+  // then iterations until no case is running (first: also tune and capture)
+  auto run_newton = [&](bool first) {
+  if (!first) CUDA_TRY(cudaMemsetAsync(h->it_ctr.p, 0, sizeof(int), st));
   ev = tm.begin(FAM_MIS);
   launch_mismatch_nr<T>(d, rg, st, x, A, max_it > 0);
   ++nl;
@@ -1046,15 +1102,13 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
   ev = tm.begin(FAM_OTHER);
   check(h, st, 0, max_it, &nl);
   tm.end(ev);
-  static const int kFam[4] = {FAM_FACT, FAM_SOLVE, FAM_UPD, FAM_MIS};
   int it = 0;
   // pick the factorisation kernels of this batch size (first solve only), before
   // the iteration is captured
-  if (h->opt.autotune && max_it > 0 && any_active(h, st)) {
+  if (first && h->opt.autotune && max_it > 0 && any_active(h, st)) {
     tune_factor<T>(J, h->ngroups, A, pan, cb, cbr, x, d.status, d.group_active, st);
     tune_bsolve<T>(J, h->ngroups, pan, x, d.group_active, st);
   }
-  auto& gph = h->nr_graph[P];
   if (h->opt.use_graph) {
     // the captured kernels hold every device pointer of d by value: capture again
     // when any of them (or the LU buffers) changed since
@@ -1092,8 +1146,27 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
     }
     ++it;
   }
+  it_total += it;
+  };
+  run_newton(true);
+  // reactive limits: switch the violating PV buses of converged cases to PQ and run
+  // those cases again from their voltages, until no case has a new violation
+  if (h->nsw > 0 && max_it > 0) {
+    const size_t tot = (size_t)h->ngroups * h->nsw * 32;
+    const int lanes = h->ngroups * 32;
+    for (int round = 0; round < kMaxQRounds; ++round) {
+      CUDA_TRY(cudaMemsetAsync(h->any_active.p, 0, sizeof(int), st));
+      k_qlim_check<<<(unsigned)std::min<size_t>(148 * 8, tot / 256 + 1), 256, 0, st>>>(
+          d, h->sw_bus.as<int>(), h->q_lim.as<double2>(), h->q_flag.as<int>());
+      k_qlim_restart<<<(lanes + 255) / 256, 256, 0, st>>>(d, h->q_flag.as<int>());
+      CUDA_TRY(cudaGetLastError());
+      nl += 2;
+      if (!any_active(h, st)) break;
+      run_newton(false);
+    }
+  }
   h->timing.launches = nl;
-  h->timing.iterations_max = it;
+  h->timing.iterations_max = it_total;
 }
 
 template <typename T>
@@ -1407,26 +1480,12 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
       upload(h->sbus0, sb);
       upload(h->v0, v0);
       upload(h->mis_rows, g.mis_rows);
-      std::vector<int2> jv(g.nb);
-      for (int i = 0; i < g.nb; ++i) jv[i] = make_int2(g.var_va[i], g.var_vm[i]);
-      upload(h->jvar, jv);
-      std::vector<int4> jp(g.y_col.size());
-      for (size_t p = 0; p < jp.size(); ++p)
-        jp[p] = make_int4(g.jpos[4 * p], g.jpos[4 * p + 1], g.jpos[4 * p + 2], g.jpos[4 * p + 3]);
-      upload(h->jpos, jp);
     }
     if (g.n_islands > 1) {
-      std::vector<int> vi(g.jac.n, -1);
-      for (int i = 0; i < g.nb; ++i) {
-        if (g.var_va[i] >= 0) vi[g.var_va[i]] = g.bus_island[i];
-        if (g.var_vm[i] >= 0) vi[g.var_vm[i]] = g.bus_island[i];
-      }
-      h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac, &vi);
       upload(h->bus_island, g.bus_island);
       upload(h->br_island, g.br_island);
-    } else {
-      h->jac.setup(g.jac, g.ah_ptr, g.ah_loc, g.nnz_jac);
     }
+    upload_newton(h.get());
     h->any_active.alloc(sizeof(int));
     h->it_ctr.alloc(sizeof(int));
     return MPF_OK;
@@ -1614,6 +1673,18 @@ int set_cases_impl(mpf_handle* h, int32_t n_cases, const int32_t* island_of_case
       h->bp[v].group_island = gi;
       h->bpp[v].group_island = gi;
     }
+    if (h->nsw > 0) {
+      // every limited bus starts as PV in every case
+      const size_t n = (size_t)lanes * h->nsw;
+      h->pv_on.alloc(n);
+      h->q_fix.alloc(n * sizeof(double));
+      h->q_flag.alloc((size_t)lanes * sizeof(int));
+      h->iter_base.alloc((size_t)lanes * sizeof(int));
+      CUDA_TRY(cudaMemset(h->pv_on.p, 1, n));
+      CUDA_TRY(cudaMemset(h->q_fix.p, 0, n * sizeof(double)));
+      CUDA_TRY(cudaMemset(h->q_flag.p, 0, (size_t)lanes * sizeof(int)));
+      CUDA_TRY(cudaMemset(h->iter_base.p, 0, (size_t)lanes * sizeof(int)));
+    }
     h->ncases = n_cases;
     h->ngroups = ngroups;
     h->maxk = maxk;
@@ -1771,10 +1842,88 @@ int32_t mpf_set_controls(mpf_handle* h, int32_t n_controls, const mpf_control* c
   });
 }
 
+int32_t mpf_set_q_limits(mpf_handle* h, const double* qmin, const double* qmax) {
+  if (!h) return MPF_ERR_BAD_INPUT;
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->own_stream));
+    if (h->last_stream) CUDA_TRY(cudaStreamSynchronize(h->last_stream));
+    const int nb = h->g.nb;
+    std::vector<char> vf(nb, 0);
+    std::vector<int> swi(nb, -1), swb;
+    std::vector<double2> lim;
+    for (int i = 0; i < nb && (qmin || qmax); ++i) {
+      if (h->g.bus_type[i] != MPF_BUS_PV) continue;
+      double lo = qmin ? qmin[i] : -INFINITY, hi = qmax ? qmax[i] : INFINITY;
+      if (lo != lo) lo = -INFINITY;
+      if (hi != hi) hi = INFINITY;
+      if (lo > hi) return fail(h, MPF_ERR_BAD_INPUT, "bus " + std::to_string(i) + ": qmin > qmax");
+      if (!std::isfinite(lo) && !std::isfinite(hi)) continue;
+      vf[i] = 1;
+      swi[i] = (int)swb.size();
+      swb.push_back(i);
+      lim.push_back(make_double2(lo, hi));
+    }
+    // the Newton system with a Vm variable and a Q equation for every limited PV bus
+    GridSymbolic g2;
+    const std::string msg = build_symbolic(h->buses.data(), nb, h->branches.data(), (int)h->branches.size(), g2,
+                                           swb.empty() ? nullptr : &vf);
+    if (!msg.empty()) return fail(h, MPF_ERR_BAD_INPUT, msg);
+    if (g2.jac.max_front > kFmaxAll)
+      return fail(h, MPF_ERR_BAD_INPUT, "largest frontal matrix with the limited PV buses exceeds " +
+                                            std::to_string(kFmaxAll));
+    for (int p = 0; p < 2; ++p) h->nr_graph[p].release();
+    h->jac.release_values();
+    h->jac.tuned.clear();
+    h->jac.tuned_bs.clear();
+    h->g = std::move(g2);
+    h->vm_free = vf;
+    h->nsw = (int)swb.size();
+    upload_newton(h);
+    if (h->nsw > 0) {
+      upload(h->sw_index, swi);
+      upload(h->sw_bus, swb);
+      upload(h->q_lim, lim);
+    }
+    // the batch must be defined again for the new system
+    h->have_cases = false;
+    h->have_results = false;
+    h->ngroups = 0;
+    h->ctl.clear();
+    return MPF_OK;
+  });
+}
+
+int32_t mpf_get_bus_types(mpf_handle* h, uint8_t* types) {
+  if (!h || !types) return MPF_ERR_BAD_INPUT;
+  if (!h->have_results) return fail(h, MPF_ERR_STATE, "no results: call mpf_solve first");
+  return guarded(h, [&]() -> int {
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t st = h->own_stream;
+    CUDA_TRY(cudaStreamWaitEvent(st, h->t1, 0));
+    if (!h->base_type.p) {
+      std::vector<uint8_t> bt(h->g.nb);
+      for (int i = 0; i < h->g.nb; ++i) bt[i] = (uint8_t)h->g.bus_type[i];
+      upload(h->base_type, bt);
+    }
+    const size_t total = (size_t)h->ncases * h->g.nb;
+    DevBuf out;
+    out.alloc(total);
+    k_gather_types<<<(unsigned)std::min<size_t>(148 * 16, total / 256 + 1), 256, 0, st>>>(
+        h->dev(), h->ncases, h->base_type.as<unsigned char>(), out.as<unsigned char>());
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(types, out.p, total, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return MPF_OK;
+  });
+}
+
 int32_t mpf_solve(mpf_handle* h, int32_t alg, int32_t precision, void* stream) {
   if (!h) return MPF_ERR_BAD_INPUT;
   if (!h->have_cases) return fail(h, MPF_ERR_STATE, "mpf_set_cases must be called before mpf_solve");
   if (alg != MPF_NR && alg != MPF_FDXB && alg != MPF_FDBX) return fail(h, MPF_ERR_BAD_INPUT, "unknown algorithm");
+  if (alg != MPF_NR && h->nsw > 0)
+    return fail(h, MPF_ERR_BAD_INPUT, "reactive limits are enforced with Newton-Raphson only");
   if (precision != MPF_FP64 && precision != MPF_MIXED) return fail(h, MPF_ERR_BAD_INPUT, "unknown precision");
   return guarded(h, [&]() -> int {
     CUDA_TRY(cudaSetDevice(h->device));

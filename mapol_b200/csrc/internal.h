@@ -152,8 +152,10 @@ struct GridSymbolic {
 };
 
 // Validates the grid and fills g.  Returns empty string on success, else a message.
+// vm_free (nullable): PV buses that also get a Vm variable and a Q equation (buses
+// whose reactive limits may switch them to PQ).
 std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, int nbr,
-                           GridSymbolic& g);
+                           GridSymbolic& g, const std::vector<char>* vm_free = nullptr);
 
 }  // namespace mpf
 

@@ -77,6 +77,14 @@ struct DevGrid {
   // case <-> lane when lanes are grouped by island and padded (null: lane = case)
   const int* lane_case;     // [ngroups*32] user case or -1 (padding)
   const int* case_lane;     // [ncases]
+  // reactive limits (null when not enforced): PV buses with limits have a Vm variable
+  // and a Q equation; while a bus is PV in a case its Q row is the identity, its Vm
+  // column zero and its mismatch 0, so dVm = 0 exactly
+  int nsw;                  // PV buses whose limits are enforced
+  const int* sw_index;      // [nb] index among them or -1
+  unsigned char* pv_on;     // [g][nsw][32] 1 while PV in that case, 0 once switched to PQ
+  double* q_fix;            // [g][nsw][32] Q the switched bus holds (its violated limit)
+  int* iter_base;           // [ngroups*32] Newton iterations of the case's earlier rounds
 };
 
 __device__ __forceinline__ bool row_here(const DevGrid& d, int i, int g) {
@@ -84,6 +92,12 @@ __device__ __forceinline__ bool row_here(const DevGrid& d, int i, int g) {
 }
 __device__ __forceinline__ bool branch_here(const DevGrid& d, int k, int g) {
   return !d.group_island || d.br_island[k] == d.group_island[g];
+}
+// index among the limited PV buses of bus i if it is still PV in this lane, else -1
+__device__ __forceinline__ bool still_pv(const DevGrid& d, int i, int g, int lane) {
+  if (!d.sw_index) return false;
+  const int k = d.sw_index[i];
+  return k >= 0 && d.pv_on[at32(g, d.nsw, k, lane)];
 }
 __device__ __forceinline__ int lane_of_case(const DevGrid& d, int c) { return d.case_lane ? d.case_lane[c] : c; }
 __device__ __forceinline__ int case_of_lane(const DevGrid& d, int lane, int ncases) {
@@ -259,7 +273,7 @@ __global__ void k_check(DevGrid d, int it_arg, int max_it, double tol) {
     if (d.status[c] == ST_RUNNING) {
       const double m = __longlong_as_double((long long)d.facc[c]);
       d.maxmis[c] = m;
-      d.iters[c] = it;
+      d.iters[c] = it + (d.iter_base ? d.iter_base[c] : 0);
       if (!(m <= DBL_MAX)) d.status[c] = ST_DIVERGED;
       else if (m < tol) d.status[c] = ST_CONVERGED;
       else if (it >= max_it) d.status[c] = ST_MAX_ITER;
@@ -287,24 +301,29 @@ constexpr int kRowsPerBlock = 64;
 //   dQ/dVa = -b (-I_i + yv_i) + a (I_r - yv_r)     dQ/dVm = -a w_i + b w_r + (I_r d - I_i c)/|V_j|
 // J entries of Ybus entry (i, j) of this lane's case, written at the arrowhead
 // positions jp (-1: not a J entry).  I = Ibus_i on the diagonal, 0 elsewhere.
+// qrow_off: row i's Q equation is inactive (bus i still PV); vmcol_off: column j's Vm
+// is fixed (bus j still PV).  Inactive entries are 0, the (Q_i, Vm_i) diagonal 1.
 template <typename T>
 __device__ __forceinline__ void jac_entry(const DevGrid& d, T* A, int g, int lane, int4 jp, double2 y, double2 vj,
-                                          double a, double b, double ir, double ii) {
+                                          double a, double b, double ir, double ii, bool qrow_off = false,
+                                          bool vmcol_off = false, bool diag = false) {
   const double cc = vj.x, dd = vj.y;
   const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
   if (jp.x >= 0) A[at32(g, d.nA_jac, jp.x, lane)] = (T)(-b * (ir - yvr) - a * (-ii + yvi));
-  if (jp.z >= 0) A[at32(g, d.nA_jac, jp.z, lane)] = (T)(-b * (-ii + yvi) + a * (ir - yvr));
+  if (jp.z >= 0) A[at32(g, d.nA_jac, jp.z, lane)] = qrow_off ? (T)0 : (T)(-b * (-ii + yvi) + a * (ir - yvr));
   if (jp.y >= 0 || jp.w >= 0) {
     const double inv = 1.0 / sqrt(cc * cc + dd * dd);  // 1 / |V_j|
     const double wr = yvr * inv, wi = yvi * inv;
-    if (jp.y >= 0) A[at32(g, d.nA_jac, jp.y, lane)] = (T)(a * wr + b * wi + (ir * cc + ii * dd) * inv);
-    if (jp.w >= 0) A[at32(g, d.nA_jac, jp.w, lane)] = (T)(-a * wi + b * wr + (ir * dd - ii * cc) * inv);
+    if (jp.y >= 0) A[at32(g, d.nA_jac, jp.y, lane)] = vmcol_off ? (T)0 : (T)(a * wr + b * wi + (ir * cc + ii * dd) * inv);
+    if (jp.w >= 0)
+      A[at32(g, d.nA_jac, jp.w, lane)] = (qrow_off || vmcol_off) ? (T)(qrow_off && vmcol_off && diag ? 1 : 0)
+                                                                 : (T)(-a * wi + b * wr + (ir * dd - ii * cc) * inv);
   }
 }
 
 // One pass over the row: the off-diagonal J entries need no Ibus and are written
 // while Ibus accumulates; the diagonal entry follows once Ibus is complete.
-template <typename T, bool JAC, bool CTL>
+template <typename T, bool JAC, bool CTL, bool QL>
 __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
   const int g = blockIdx.y;
   if (!d.group_active[g]) return;
@@ -321,6 +340,7 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
     const int p0 = d.y_rowptr[i], p1 = d.y_rowptr[i + 1];
     const bool touched = row_touched(o, d.y_diag[i]);
     const double2 vi = d.V[at32(g, d.nb, i, lane)];
+    const bool pvi = QL && still_pv(d, i, g, lane);
     for (int p = p0; p < p1; ++p) {
       const int j = d.y_col[p];
       const double2 y = yentry<CTL>(d, o, touched, p, g, lane);
@@ -329,17 +349,21 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
       ib.y += y.x * v.y + y.y * v.x;
       if (JAC && j != i) {
         const int4 jp = d.jpos[p];
-        if (jp.x >= 0 || jp.y >= 0 || jp.z >= 0 || jp.w >= 0) jac_entry<T>(d, A, g, lane, jp, y, v, vi.x, vi.y, 0.0, 0.0);
+        if (jp.x >= 0 || jp.y >= 0 || jp.z >= 0 || jp.w >= 0)
+          jac_entry<T>(d, A, g, lane, jp, y, v, vi.x, vi.y, 0.0, 0.0, pvi, QL && still_pv(d, j, g, lane));
       }
     }
-    const double2 s = d.sbus_case ? d.sbus_case[at32(g, d.nb, i, lane)] : d.sbus0[i];
+    double2 s = d.sbus_case ? d.sbus_case[at32(g, d.nb, i, lane)] : d.sbus0[i];
+    if (QL && !pvi && d.sw_index[i] >= 0) s.y = d.q_fix[at32(g, d.nsw, d.sw_index[i], lane)];
     // mis = V conj(Ibus) - S
     const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
     const double mi = vi.y * ib.x - vi.x * ib.y - s.y;
     const int2 jv = d.jvar[i];
     x[at32(g, d.n_jac, jv.x, lane)] = (T)mr;
     double m = fabs(mr);
-    if (jv.y >= 0) {
+    if (jv.y >= 0 && pvi) {
+      x[at32(g, d.n_jac, jv.y, lane)] = (T)0;  // Q of a PV bus is free: its row asks dVm = 0
+    } else if (jv.y >= 0) {
       x[at32(g, d.n_jac, jv.y, lane)] = (T)mi;
       m = fmax(m, fabs(mi));
       if (mi != mi) m = INFINITY;
@@ -349,7 +373,8 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
     if (JAC) {
       const int pd = d.y_diag[i];
       const int4 jp = d.jpos[pd];
-      jac_entry<T>(d, A, g, lane, jp, yentry<CTL>(d, o, touched, pd, g, lane), vi, vi.x, vi.y, ib.x, ib.y);
+      jac_entry<T>(d, A, g, lane, jp, yentry<CTL>(d, o, touched, pd, g, lane), vi, vi.x, vi.y, ib.x, ib.y, pvi, pvi,
+                   true);
     } else {
       d.Ibus[at32(g, d.nb, i, lane)] = ib;
     }
@@ -1002,12 +1027,14 @@ __global__ void __launch_bounds__(256) k_mismatch_eval(DevGrid d, const double2*
       ib.y += y.x * vj.y + y.y * vj.x;
     }
     const double2 vi = vc[i];
-    const double2 s = d.sbus_case ? d.sbus_case[at32(ln >> 5, d.nb, i, ln & 31)] : d.sbus0[i];
+    double2 s = d.sbus_case ? d.sbus_case[at32(ln >> 5, d.nb, i, ln & 31)] : d.sbus0[i];
+    const bool pvi = still_pv(d, i, ln >> 5, ln & 31);
+    if (d.sw_index && !pvi && d.sw_index[i] >= 0) s.y = d.q_fix[at32(ln >> 5, d.nsw, d.sw_index[i], ln & 31)];
     const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
     const double mi = vi.y * ib.x - vi.x * ib.y - s.y;
     m = fabs(mr);
     if (mr != mr) m = INFINITY;
-    if (d.jvar[i].y >= 0) {
+    if (d.jvar[i].y >= 0 && !pvi) {
       m = fmax(m, fabs(mi));
       if (mi != mi) m = INFINITY;
     }
@@ -1127,8 +1154,8 @@ __global__ void __launch_bounds__(256) k_adj_dldx(DevGrid d, int nbr, const doub
     const int2 vfv = d.jvar[ft.x], vtv = d.jvar[ft.y];
     if (vfv.x >= 0) atomicAdd(&g[at32(grp, d.n_jac, vfv.x, lane)], (T)(-cc * swi));
     if (vtv.x >= 0) atomicAdd(&g[at32(grp, d.n_jac, vtv.x, lane)], (T)(cc * swi));
-    if (vfv.y >= 0) atomicAdd(&g[at32(grp, d.n_jac, vfv.y, lane)], (T)dvm_f);
-    if (vtv.y >= 0) atomicAdd(&g[at32(grp, d.n_jac, vtv.y, lane)], (T)(cc * swr / mt));
+    if (vfv.y >= 0 && !still_pv(d, ft.x, grp, lane)) atomicAdd(&g[at32(grp, d.n_jac, vfv.y, lane)], (T)dvm_f);
+    if (vtv.y >= 0 && !still_pv(d, ft.y, grp, lane)) atomicAdd(&g[at32(grp, d.n_jac, vtv.y, lane)], (T)(cc * swr / mt));
   }
 }
 
@@ -1215,7 +1242,7 @@ __global__ void k_adj_grad_bus(DevGrid d, int ncases, const T* __restrict__ lam,
     const int2 jv = d.jvar[i];
     const bool ok = d.status[c] == ST_CONVERGED && row_here(d, i, c >> 5);
     if (gp) gp[t] = (ok && jv.x >= 0) ? (double)lam[at32(c >> 5, d.n_jac, jv.x, c & 31)] : 0.0;
-    if (gq) gq[t] = (ok && jv.y >= 0) ? (double)lam[at32(c >> 5, d.n_jac, jv.y, c & 31)] : 0.0;
+    if (gq) gq[t] = (ok && jv.y >= 0 && !still_pv(d, i, c >> 5, c & 31)) ? (double)lam[at32(c >> 5, d.n_jac, jv.y, c & 31)] : 0.0;
   }
 }
 
@@ -1410,6 +1437,83 @@ __global__ void k_fd_ctl(DevGrid d, DevCtl t, int variant, int nA, const int* __
     }
     const size_t idx = at32(g, nA, pos, lane);
     A[idx] = (T)((double)A[idx] + acc);
+  }
+}
+
+// ---------------------------------------------------------------- reactive limits
+// Start of a solve: every limited bus is PV in every case, no earlier rounds.
+__global__ void k_qlim_reset(DevGrid d) {
+  const size_t total = (size_t)d.ngroups * 32 * d.nsw;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x)
+    d.pv_on[t] = 1;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.ngroups * 32; c += gridDim.x * blockDim.x)
+    d.iter_base[c] = 0;
+}
+
+// After a Newton run: for every converged case and every bus still PV there, the net
+// reactive injection Q = Im(V_i conj(Ibus_i)); outside [qmin, qmax] the bus becomes PQ
+// holding the violated limit (all violators of a case at once, as MATPOWER's runpf with
+// ENFORCE_Q_LIMS = 1) and the case is flagged for another run.  Thread per (bus, lane).
+__global__ void k_qlim_check(DevGrid d, const int* __restrict__ sw_bus, const double2* __restrict__ q_lim,
+                             int* __restrict__ flag) {
+  const size_t total = (size_t)d.ngroups * d.nsw * 32;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int lane = (int)(t & 31);
+    const size_t rest = t >> 5;
+    const int k = (int)(rest % d.nsw), g = (int)(rest / d.nsw);
+    const int c = g * 32 + lane;
+    const size_t sk = at32(g, d.nsw, k, lane);
+    const int i = sw_bus[k];
+    if (d.status[c] != ST_CONVERGED || !d.pv_on[sk] || !row_here(d, i, g)) continue;
+    LaneOut o;
+    load_outages(d, c, o);
+    const bool touched = row_touched(o, d.y_diag[i]);
+    double2 ib = make_double2(0.0, 0.0);
+    for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
+      const double2 y = yentry(d, o, touched, p, g, lane);
+      const double2 v = d.V[at32(g, d.nb, d.y_col[p], lane)];
+      ib.x += y.x * v.x - y.y * v.y;
+      ib.y += y.x * v.y + y.y * v.x;
+    }
+    const double2 vi = d.V[at32(g, d.nb, i, lane)];
+    const double q = vi.y * ib.x - vi.x * ib.y;
+    const double2 lim = q_lim[k];
+    if (q > lim.y || q < lim.x) {
+      d.pv_on[sk] = 0;
+      d.q_fix[sk] = q > lim.y ? lim.y : lim.x;
+      flag[c] = 1;
+    }
+  }
+}
+
+// Flagged cases run Newton again from their voltages; the others keep their status.
+__global__ void k_qlim_restart(DevGrid d, int* __restrict__ flag) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nl = d.ngroups * 32;
+  bool again = false;
+  if (c < nl && flag[c]) {
+    flag[c] = 0;
+    d.iter_base[c] = d.iters[c];
+    d.status[c] = ST_RUNNING;
+    again = true;
+  }
+  const unsigned any = __ballot_sync(0xffffffffu, again);
+  if ((threadIdx.x & 31) == 0 && c < nl) {
+    d.group_active[c >> 5] = any != 0u;
+    if (any) atomicAdd(d.any_active, 1);
+  }
+}
+
+// [group][..][32] bus types after the limits: a switched PV bus reads PQ.
+__global__ void k_gather_types(DevGrid d, int ncases, const unsigned char* __restrict__ base_type,
+                               unsigned char* __restrict__ out) {
+  const size_t total = (size_t)ncases * d.nb;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int uc = (int)(t / d.nb), i = (int)(t % d.nb);
+    const int c = lane_of_case(d, uc);
+    unsigned char ty = base_type[i];
+    if (d.sw_index && d.sw_index[i] >= 0 && !d.pv_on[at32(c >> 5, d.nsw, d.sw_index[i], c & 31)]) ty = 1;
+    out[t] = ty;
   }
 }
 

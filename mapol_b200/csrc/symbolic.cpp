@@ -377,7 +377,7 @@ static void build_fd(GridSymbolic& g, const mpf_bus* buses, const mpf_branch* br
 }
 
 std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, int nbr,
-                           GridSymbolic& g) {
+                           GridSymbolic& g, const std::vector<char>* vm_free) {
   g = GridSymbolic();
   if (nb < 2) return "grid needs at least 2 buses";
   if (nbr < 1) return "grid needs at least 1 branch";
@@ -567,7 +567,10 @@ std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, i
     const int i = free_bus[border[k]];
     g.bus_order[k] = i;
     g.var_va[i] = nv++;
-    if (g.bus_type[i] == MPF_BUS_PQ) g.var_vm[i] = nv++;
+    // Vm is a variable of every PQ bus, and of PV buses that may switch to PQ (their
+    // Q limits are enforced): a superset pattern shared by all cases
+    if (g.bus_type[i] == MPF_BUS_PQ || (vm_free && (*vm_free)[i] && g.bus_type[i] == MPF_BUS_PV))
+      g.var_vm[i] = nv++;
   }
   // variable adjacency
   std::vector<std::vector<int>> vadj(nv);

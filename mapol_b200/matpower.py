@@ -11,7 +11,9 @@ Follows the reference's loader (src/files/loadMatpowerFormat.h:14-209):
 Differences, stated: the generator voltage set-point VG becomes the PV/slack bus
 magnitude (the reference stores VG in Bus::VG and its optimiser starts AVR controls
 from it, main.cu:276-395; MATPOWER's runpf does the same), and branch rating A
-(MVA, returned as p.u.) is kept where the reference discards it.
+(MVA, returned as p.u.) is kept where the reference discards it.  q_limits()
+returns the generators' reactive limits, which the reference parses
+(loadMatpowerFormat.h:130-137) and never uses, as net-injection limits per bus.
 """
 import re
 
@@ -71,3 +73,31 @@ def load_matpower(path):
         branches[k]["shift"] = r[9]
         branches[k]["status"] = 1 if r[10] != 0 else 0
     return buses, branches, rating
+
+
+def q_limits(path):
+    """(qmin, qmax) per bus in p.u. of net reactive injection: the sum of the Qmin /
+    Qmax of the bus's generators (gen columns 5 and 4) minus its reactive load Qd;
+    -inf / +inf at buses without generators or with infinite limits."""
+    with open(path) as f:
+        text = f.read()
+    base = float(re.search(r"mpc\.baseMVA\s*=\s*([0-9.eE+-]+)", text).group(1))
+    bus = _matrix(text, "bus")
+    gen = _matrix(text, "gen") or []
+    ids = {int(r[0]): i for i, r in enumerate(bus)}
+    nb = len(bus)
+    qmin = np.full(nb, -np.inf)
+    qmax = np.full(nb, np.inf)
+    has = np.zeros(nb, bool)
+    sum_min = np.zeros(nb)
+    sum_max = np.zeros(nb)
+    for r in gen:
+        i = ids[int(r[0])]
+        has[i] = True
+        sum_max[i] += r[3]
+        sum_min[i] += r[4]
+    for i, r in enumerate(bus):
+        if has[i]:
+            qmax[i] = (sum_max[i] - r[3]) / base
+            qmin[i] = (sum_min[i] - r[3]) / base
+    return qmin, qmax

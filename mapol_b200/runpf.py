@@ -102,6 +102,23 @@ class PowerFlow:
             self._check(lib().mpf_set_cases_islands(self._h, len(cases), ptr(isl), ptr(offs), ptr(flat), ptr(sb)))
         self.n_cases = len(cases)
 
+    def set_q_limits(self, qmin, qmax):
+        """Reactive limits of PV buses (mpf_set_q_limits): per-bus net-injection limits in
+        p.u., +-inf / NaN for none; None for both disables.  Call before set_cases."""
+        lo = None if qmin is None else np.ascontiguousarray(qmin, dtype=np.float64)
+        hi = None if qmax is None else np.ascontiguousarray(qmax, dtype=np.float64)
+        for a in (lo, hi):
+            if a is not None and a.shape != (len(self.buses),):
+                raise ValueError("limits need one entry per bus")
+        self._check(lib().mpf_set_q_limits(self._h, ptr(lo), ptr(hi)))
+        self.n_cases = 0
+
+    def bus_types(self):
+        """(n_cases, n_bus) bus types after the last solve (switched PV buses read PQ)."""
+        out = np.zeros((self.n_cases, len(self.buses)), np.uint8)
+        self._check(lib().mpf_get_bus_types(self._h, ptr(out)))
+        return out
+
     def set_controls(self, controls, values):
         """Per-case control overrides of the current cases (mpf_set_controls).
         controls: sequence of (kind, index) with kind CTRL_AVR (PV/slack bus |V|

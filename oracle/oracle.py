@@ -119,3 +119,52 @@ def loss(buses, branches, v, outages=()):
     out = np.asarray(list(outages) + [0], np.int32)
     vv = np.stack([v.real, v.imag], -1).astype(np.float64).copy()
     return L.oracle_loss(_p(buses), len(buses), _p(branches), len(branches), _p(out), len(outages), _p(vv))
+
+
+def runpf_qlim(buses, branches, cases, qmin, qmax, alg=0, tol=1e-8, sbus=None, max_rounds=20, solver=SOLVER_GP):
+    """Newton-Raphson with reactive limits of PV buses, case by case (MATPOWER runpf
+    with ENFORCE_Q_LIMS = 1; the reference parses the limits but never enforces them,
+    loadMatpowerFormat.h:130-137): solve; at the converged voltages compute each PV
+    bus's net reactive injection Q = Im(V_i conj((Ybus V)_i)); every PV bus outside
+    [qmin, qmax] becomes PQ with Q at the violated limit; solve again; repeat until no
+    new violation.  Each round solves from the start point (runpf.h:211-226) with the
+    updated bus types, which converges to the same state as continuing from the
+    previous round's voltages.  Returns dict(v, converged, iterations (summed over the
+    rounds), switched (bool, n_cases x n_bus), rounds)."""
+    nb = len(buses)
+    n = len(cases)
+    lo = np.where(np.isnan(qmin), -np.inf, qmin)
+    hi = np.where(np.isnan(qmax), np.inf, qmax)
+    out_v = np.zeros((n, nb), complex)
+    conv = np.zeros(n, bool)
+    iters = np.zeros(n, np.int32)
+    switched = np.zeros((n, nb), bool)
+    rounds = np.zeros(n, np.int32)
+    for c in range(n):
+        b = np.array(buses).copy()
+        sb = None if sbus is None else np.array(sbus[c:c + 1]).copy()
+        for rnd in range(max_rounds + 1):
+            r = runpf(b, branches, [cases[c]], alg=alg, tol=tol, sbus=sb, solver=solver, threads=1)
+            iters[c] += r["iterations"][0]
+            out_v[c] = r["v"][0]
+            conv[c] = r["converged"][0]
+            if not conv[c] or rnd == max_rounds:
+                break
+            ptr_, col, val = ybus(b, branches, cases[c])
+            v = r["v"][0]
+            ib = np.array([np.dot(val[ptr_[i]:ptr_[i + 1]], v[col[ptr_[i]:ptr_[i + 1]]]) for i in range(nb)])
+            q = (v * np.conj(ib)).imag
+            pv = b["type"] == 2
+            over = pv & (q > hi)
+            under = pv & (q < lo)
+            if not (over | under).any():
+                break
+            rounds[c] += 1
+            for i in np.where(over | under)[0]:
+                lim = hi[i] if over[i] else lo[i]
+                b["type"][i] = 1
+                b["q"][i] = lim
+                if sb is not None:
+                    sb[0, i, 1] = lim
+                switched[c, i] = True
+    return dict(v=out_v, converged=conv, iterations=iters, switched=switched, rounds=rounds)

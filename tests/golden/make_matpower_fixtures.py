@@ -1,7 +1,8 @@
 """Converts the reference's bundled MATPOWER cases (src/datasets/case14, 30, 118, 300)
-with mapol_b200.matpower.load_matpower into tests/golden/matpower_cases.npz, so the
-GPU tests can run real grids where the reference tree is absent.  Run from the
-repository root:  python tests/golden/make_matpower_fixtures.py
+with mapol_b200.matpower.load_matpower (and the generators' Q limits, q_limits) into
+tests/golden/matpower_cases.npz, so the GPU tests can run real grids where the reference
+tree is absent.  Run from the repository root:
+python tests/golden/make_matpower_fixtures.py
 """
 import os
 import sys
@@ -11,7 +12,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from mapol_b200.matpower import load_matpower  # noqa: E402
+from mapol_b200.matpower import load_matpower, q_limits  # noqa: E402
 
 SRC = "/root/reference/src/datasets"
 
@@ -23,6 +24,7 @@ def main():
         out[name + "_buses"] = buses
         out[name + "_branches"] = branches
         out[name + "_rating"] = rating
+        out[name + "_qmin"], out[name + "_qmax"] = q_limits(os.path.join(SRC, name + ".m"))
     np.savez_compressed(os.path.join(ROOT, "tests", "golden", "matpower_cases.npz"), **out)
 
 

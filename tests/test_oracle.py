@@ -115,3 +115,35 @@ def test_golden_fixtures_reproduced():
             assert np.array_equal(r["iterations"], g[f"{name}_{tag}_iterations"])
             assert np.array_equal(r["converged"], g[f"{name}_{tag}_converged"])
             assert np.abs(r["v"] - g[f"{name}_{tag}_v"]).max() < 1e-12
+
+
+def test_qlim_oracle_switches_and_holds_the_limit():
+    """runpf_qlim on the IEEE 14-bus case: limits that never bind change nothing; a
+    limit just below a PV bus's solved Q switches it to PQ, where its Q then equals
+    the limit and its |V| leaves the set-point."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "matpower_cases.npz"))
+    b, br = g["case14_buses"], g["case14_branches"]
+    nb = len(b)
+    base = oracle.runpf(b, br, [[]], alg=0)
+    wide = oracle.runpf_qlim(b, br, [[]], np.full(nb, -np.inf), np.full(nb, np.inf))
+    assert not wide["switched"].any() and np.array_equal(wide["v"], base["v"])
+    v = base["v"][0]
+    ptr, col, val = oracle.ybus(b, br)
+    ib = np.array([np.dot(val[ptr[i]:ptr[i + 1]], v[col[ptr[i]:ptr[i + 1]]]) for i in range(nb)])
+    q = (v * np.conj(ib)).imag
+    pv = np.where(b["type"] == 2)[0]
+    k = pv[np.argmax(q[pv])]
+    qmax = np.full(nb, np.inf)
+    qmax[k] = q[k] - 0.05
+    r = oracle.runpf_qlim(b, br, [[]], np.full(nb, -np.inf), qmax)
+    assert r["converged"][0] and r["switched"][0, k] and r["switched"][0].sum() == 1
+    v2 = r["v"][0]
+    bb = b.copy()
+    bb["type"][k] = 1
+    bb["q"][k] = qmax[k]
+    ptr, col, val = oracle.ybus(bb, br)
+    ib2 = np.array([np.dot(val[ptr[i]:ptr[i + 1]], v2[col[ptr[i]:ptr[i + 1]]]) for i in range(nb)])
+    assert abs((v2[k] * np.conj(ib2[k])).imag - qmax[k]) < 1e-9
+    assert abs(abs(v2[k]) - b["vm"][k]) > 1e-4
