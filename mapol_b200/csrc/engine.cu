@@ -284,6 +284,9 @@ void ensure_attrs(int device) {
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 32, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G / 2, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 16, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 16, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 8, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
@@ -332,6 +335,7 @@ template <typename T>
 void launch_factor_ge(int ge, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr,
                       T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
   switch (ge) {
+    case 16: launch_factor_one<T, 16, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
     case 8: launch_factor_one<T, 8, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
     case 4: launch_factor_one<T, 4, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
     case 2: launch_factor_one<T, 2, 256>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1); break;
@@ -435,11 +439,16 @@ std::vector<FactorChoice> factor_candidates(const Launch& ln, int ngroups) {
   }
   for (int tpb : {8, 4, 2})
     if (factor_smem_rt(ln.fcap, G, tpb, 0, ws) <= kSmemMax) add({0, G, 0, tpb});
-  // half-width lane chunks: half the shared memory per warp, twice the resident warps
-  if (ln.fcap <= kFmaxM)
+  // half-width lane chunks: half the shared memory per warp, twice the resident warps;
+  // 16 lanes: wider contiguous accesses, fewer resident teams
+  if (ln.fcap <= kFmaxM) {
     for (int tpb : {8, 4})
       if (factor_smem_rt(ln.fcap, G / 2, tpb, 0, ws) <= kSmemMax) add({0, G / 2, 0, tpb});
-  for (int ge = G; ge >= 1; ge /= 2)
+    if (G != 16)
+      for (int tpb : {4, 2})
+        if (factor_smem_rt(ln.fcap, 16, tpb, 0, ws) <= kSmemMax) add({0, 16, 0, tpb});
+  }
+  for (int ge = 16; ge >= 1; ge /= 2)
     if (factor_smem_rt(ln.fcap, ge, 1, 0, ws) <= kSmemMax) add({1, ge, 0, 1});
   const int tt = reg_tt(ln.fcap);
   if (ln.fcap > kFmaxS && tt <= kRegTTMax)
@@ -460,6 +469,8 @@ void launch_choice(const FactorChoice& ch, const LUSystem& sys, const Launch& ln
     else if (ch.ge == G / 2)
       launch_factor_one<T, G / 2, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st,
                                       ch.tpb);
+    else if (ch.ge == 16)
+      launch_factor_one<T, 16, 32>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, ch.tpb);
     else
       throw MpfError{MPF_ERR_INTERNAL, "no warp-team kernel for this lane count"};
   } else if (ch.kind == 1) {
@@ -581,6 +592,7 @@ void launch_bsolve_one(int ge, const LUSystem& sys, const Launch& ln, int ngroup
   const size_t smem = (size_t)4 * ln.fcap * (ge ? ge : 32) * sizeof(T);
   switch (ge) {
     case 0: k_mf_bsolve<T><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 16: k_mf_bsolve_chunk<T, 16><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
     case 8: k_mf_bsolve_chunk<T, 8><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
     case 4: k_mf_bsolve_chunk<T, 4><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
     case 2: k_mf_bsolve_chunk<T, 2><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
@@ -643,7 +655,7 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
       const Launch& ln = sys.level_sched[k];
       const int h0 = bsolve_heuristic<T>(ln, ngroups);
       std::vector<int> cands{h0};
-      for (int ge : {0, 8, 4, 2, 1})
+      for (int ge : {0, 16, 8, 4, 2, 1})
         if (ge != h0) cands.push_back(ge);
       float bt = 0.0f, ht = 0.0f;
       for (size_t i = 0; i < cands.size(); ++i) {
