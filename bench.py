@@ -463,6 +463,112 @@ def run_multigrid(args, rank, world, local_rank):
     }
 
 
+def run_extras(args):
+    """Throughput of the paths beside the headline, each through the public API:
+    particle-swarm fitness evaluations (the reference's hybrid_runpf workflow on the
+    IEEE 300-bus case with its AVR / OLTC / ShC structures), N-1 solves with generator
+    reactive limits enforced, and adjoint gradients of the overload loss (1354-bus grid,
+    4096 load scenarios).  Each: warm-up, then timed runs on the device clock."""
+    import torch
+
+    import mapol_b200 as m
+    from mapol_b200 import pso
+    from oracle import oracle
+
+    g = np.load(os.path.join(ROOT, "tests", "golden", "matpower_cases.npz"))
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) / reps
+
+    out = {"metric": "extras: PSO fitness evaluations/s, Q-limited N-1 solves/s, adjoint gradients/s",
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup}
+    # particle swarm: 1024 particles, fitness = active loss or DBL_MAX (runpf.h:748-791)
+    buses, branches = g["case300_buses"], g["case300_branches"]
+    est, bie, rie = pso.estruturas(buses, branches)
+    rng = np.random.default_rng(0)
+    lo = np.array([e.min for e in est])
+    hi = np.array([e.max for e in est])
+    X = lo + (hi - lo) * rng.random((1024, len(est)))
+    enxame = [pso.Particula(x) for x in X]
+    eng = pso.hybrid_init(buses, branches, len(enxame), 1, est, m.NR, bie, rie, precision=m.MIXED)
+    dt = timed(lambda: pso.hybrid_runpf(eng, est, enxame), args.steps)
+    fit = np.array([p.fitness for p in enxame])
+    pso.hybrid_free(eng)
+    controls, cols = pso.bind(est, bie, rie, branches)
+    n_cpu = min(64, len(enxame))
+    t = time.perf_counter()
+    for c in range(n_cpu):
+        b, br = buses.copy(), branches.copy()
+        for (kind, idx), v in zip(controls, X[c, cols]):
+            if kind == m.CTRL_AVR:
+                b["vm"][idx] = v
+            elif kind == m.CTRL_SHC:
+                b["bsh"][idx] = v
+            else:
+                br["tap"][idx] = v
+        oracle.runpf(b, br, [[]], alg=0, threads=1)
+    dt_cpu = (time.perf_counter() - t) / n_cpu
+    out["pso"] = {"grid": "IEEE 300-bus (reference's case300.m)", "particles": len(enxame),
+                  "structures": len(est), "value": len(enxame) / dt, "unit": "fitness evaluations/s",
+                  "ms_per_swarm": dt * 1e3, "feasible": int((fit < pso.DBL_MAX).sum()),
+                  "cpu_oracle_one_thread": {"value": 1.0 / dt_cpu, "unit": "fitness evaluations/s",
+                                            "sample": f"{n_cpu} particles, NR FP64, one host thread"}}
+    # generator reactive limits on the IEEE 300-bus case, N-1
+    cases = m.n1_cases(branches, len(buses), 256, 5, with_base=True)
+    res = {}
+    for lim in (False, True):
+        with m.PowerFlow(buses, branches) as pf:
+            if lim:
+                pf.set_q_limits(g["case300_qmin"], g["case300_qmax"])
+            pf.set_cases(cases)
+            dt = timed(lambda: pf.solve(m.NR, m.MIXED, stream.cuda_stream), args.steps)
+            r = pf.results()
+            res[lim] = (len(cases) / dt, int(r.converged.sum()),
+                        int(((pf.bus_types() == 1) & (buses["type"] == 2)[None]).sum()) if lim else 0)
+    out["q_limits"] = {"grid": "IEEE 300-bus, generator Q limits of case300.m", "cases": len(cases),
+                       "value": res[True][0], "unit": "solves/s", "without_limits": res[False][0],
+                       "converged": res[True][1], "switched_buses_total": res[True][2]}
+    # adjoint on the 1354-bus grid, 4096 load scenarios
+    b4, br4, _ = m.workload("cfg4_1354bus")
+    sb = m.load_scenarios(b4, 4096, 0.05, 11)
+    with m.PowerFlow(b4, br4) as pf:
+        pf.set_cases([[]])
+        pf.solve(m.NR, m.FP64)
+        rating = 1.2 * np.abs(pf.branch_flows(flows=True)["sf"][0])
+        pf.set_ratings(rating)
+        pf.set_cases([[]] * 4096, sbus=sb)
+        pf.solve(m.NR, m.MIXED, stream.cuda_stream)
+        dt_s = timed(lambda: pf.solve(m.NR, m.MIXED, stream.cuda_stream), args.steps)
+        from mapol_b200._lib import lib
+
+        dev = torch.device("cuda")
+        gp = torch.empty((4096, len(b4)), dtype=torch.float64, device=dev)
+        gq = torch.empty_like(gp)
+        gg = torch.empty((4096, len(br4)), dtype=torch.float64, device=dev)
+        gb = torch.empty_like(gg)
+
+        def adj():
+            rc = lib().mpf_adjoint(pf._h, m.MIXED, gp.data_ptr(), gq.data_ptr(), gg.data_ptr(), gb.data_ptr(),
+                                   None)
+            if rc != 0:
+                raise RuntimeError(lib().mpf_last_error(pf._h).decode())
+
+        dt_a = timed(adj, args.steps)
+    out["adjoint"] = {"grid": "1354-bus synthetic, 4096 load scenarios", "solve_ms": dt_s * 1e3,
+                      "adjoint_ms": dt_a * 1e3, "value": 4096 / dt_a, "unit": "gradients/s (per scenario)",
+                      "note": "mpf_adjoint into device buffers: refactorisation at the solution (FP32), U^T "
+                              "and L^T substitutions, gradients w.r.t. P, Q, g, b"}
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -484,6 +590,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from mapol_b200.grid import WORKLOAD_SETS
 
+    if args.workload == "extras":
+        if rank == 0:
+            print(json.dumps(run_extras(args)), flush=True)
+        return 0
     if args.workload in WORKLOAD_SETS:
         line = run_multigrid(args, rank, world, local_rank)
     else:
