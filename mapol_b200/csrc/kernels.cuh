@@ -657,7 +657,7 @@ __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int
 // TT > 0: the partial LU runs in registers (lu_registers; TEAM 256 with one thread
 // per entry-lane group, i.e. G <= 16 bytes of lanes); TT = 0: in shared memory.
 template <typename T, int G, int TEAM, int TT = 0>
-__global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : 4) k_mf_factor(
+__global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 256 ? 1 : 4)) k_mf_factor(
     DevLU L, const int* __restrict__ task_sn, int nsn_l, int ngroups, int fcap,
     const T* __restrict__ A, T* __restrict__ pan, T* __restrict__ cb, T* __restrict__ cbr,
     T* __restrict__ x, int* __restrict__ status, const int* __restrict__ group_active, int with_rhs) {
