@@ -123,7 +123,7 @@ struct FactorChoice {
 struct LUSystem {
   LUSymbolic sym;
   DevBuf sn_w, sn_f, sn_rptr, sn_rows, child_ptr, child_list, sn_parent, rel_ptr, relmap, ah_ptr, ah_loc;
-  DevBuf pan_off, cb_off, cbr_off, lev_sn;
+  DevBuf pan_off, cb_off, cbr_off, lev_sn, child_ref;
   DevBuf sn_island;                  // multi-island handles only
   const int* group_island = nullptr; // the handle's current per-group islands (or null)
   std::vector<Launch> factor_sched;  // ascending levels
@@ -133,6 +133,7 @@ struct LUSystem {
   // autotuned lane count of every backward-solve level launch (0 = one case per thread)
   std::map<std::pair<int, int>, std::vector<int>> tuned_bs;
   std::vector<Launch> level_sched;   // one launch per level (solves), ascending
+  std::vector<int> ah_host;          // arrowhead ranges (host copy of ah_ptr)
   int nA = 0;
   // values per precision [0] = FP64, [1] = FP32
   DevBuf A[2], pan[2], cb[2], cbr[2], x[2];
@@ -160,6 +161,7 @@ struct LUSystem {
     d.pan_off = pan_off.as<long long>();
     d.cb_off = cb_off.as<long long>();
     d.cbr_off = cbr_off.as<long long>();
+    d.child_ref = child_ref.as<ChildRef>();
     d.sn_island = group_island ? sn_island.as<int>() : nullptr;
     d.group_island = group_island;
     return d;
@@ -191,12 +193,19 @@ struct LUSystem {
     upload(relmap, s.relmap);
     upload(ah_ptr, ahp);
     upload(ah_loc, ahl);
+    ah_host = ahp;
     std::vector<long long> po(s.pan_off.begin(), s.pan_off.end()), co(s.cb_off.begin(), s.cb_off.end()),
         ro(s.cbr_off.begin(), s.cbr_off.end());
     upload(pan_off, po);
     upload(cb_off, co);
     upload(cbr_off, ro);
     upload(lev_sn, s.lev_sn);
+    std::vector<ChildRef> cr(s.child_list.size());
+    for (size_t q = 0; q < s.child_list.size(); ++q) {
+      const int c = s.child_list[q];
+      cr[q] = ChildRef{s.cb_off[c], s.cbr_off[c], s.sn_f[c] - s.sn_w[c], s.rel_ptr[c]};
+    }
+    upload(child_ref, cr);
     fingerprint = structure_fingerprint(s);
     factor_sched.clear();
     level_sched.clear();
@@ -223,6 +232,23 @@ struct LUSystem {
         k = k2;
       }
     }
+  }
+
+  // Values one factorisation launch moves per case: arrowhead reads, children's
+  // contribution blocks read, panels and its own contribution block written.
+  int64_t launch_entries(const Launch& ln) const {
+    int64_t e = 0;
+    for (int k = ln.offset; k < ln.offset + ln.count; ++k) {
+      const int sn = sym.lev_sn[k];
+      const int64_t m = sym.sn_f[sn] - sym.sn_w[sn];
+      e += (ah_host[sn + 1] - ah_host[sn]) + (sym.pan_off[sn + 1] - sym.pan_off[sn]);
+      if (sym.sn_parent[sn] >= 0) e += m * m;
+      for (int c = sym.child_ptr[sn]; c < sym.child_ptr[sn + 1]; ++c) {
+        const int64_t mc = sym.sn_f[sym.child_list[c]] - sym.sn_w[sym.child_list[c]];
+        e += mc * mc;
+      }
+    }
+    return e;
   }
 
   void ensure_values(int prec, int ngroups) {
@@ -581,11 +607,13 @@ void tune_factor(LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, 
       best.push_back(bc);
       sum_best += bt;
       sum_heur += ht;
-      if (log)
+      if (log) {
+        const double bytes = (double)sys.launch_entries(ln) * sizeof(T) * 32.0 * ngroups;
         std::fprintf(stderr, "mpf tune: n %d fp%d groups %d launch sn %d cls %d fcap %d: %zu candidates, "
-                     "heuristic %.1f us, best %.1f us (kind %d lanes %d tile %d teams %d)\n",
+                     "heuristic %.1f us, best %.1f us (kind %d lanes %d tile %d teams %d), %.1f MB, %.0f GB/s\n",
                      sys.sym.n, (int)sizeof(T) * 8, ngroups, ln.count, ln.cls, ln.fcap, cands.size(), ht * 1e3,
-                     bt * 1e3, bc.kind, bc.ge, bc.tt, bc.tpb);
+                     bt * 1e3, bc.kind, bc.ge, bc.tt, bc.tpb, bytes * 1e-6, bytes / (bt * 1e-3) * 1e-9);
+      }
     }
     if (log)
       std::fprintf(stderr, "mpf tune: n %d fp%d groups %d total heuristic %.3f ms, tuned %.3f ms\n", sys.sym.n,
@@ -696,6 +724,18 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
       }
       sum_best += bt;
       sum_heur += ht;
+      if (log && std::getenv("MPF_TUNE_LOG")[0] == '2') {
+        // U-panel rows and the front's x values read, the pivots' x written
+        int64_t e = 0;
+        for (int q = ln.offset; q < ln.offset + ln.count; ++q) {
+          const int sn = sys.sym.lev_sn[q];
+          e += (int64_t)sys.sym.sn_w[sn] * sys.sym.sn_f[sn] + sys.sym.sn_f[sn] + sys.sym.sn_w[sn];
+        }
+        const double bytes = (double)e * sizeof(T) * 32.0 * ngroups;
+        std::fprintf(stderr, "mpf tune: n %d fp%d groups %d bsolve level %d sn %d fcap %d: heuristic %.1f us, "
+                     "best %.1f us (lanes %d), %.1f MB, %.0f GB/s\n", sys.sym.n, (int)sizeof(T) * 8, ngroups, k,
+                     ln.count, ln.fcap, ht * 1e3, bt * 1e3, best[k], bytes * 1e-6, bytes / (bt * 1e-3) * 1e-9);
+      }
     }
     if (log)
       std::fprintf(stderr, "mpf tune: n %d fp%d groups %d backward solve heuristic %.3f ms, tuned %.3f ms\n",

@@ -104,6 +104,13 @@ __device__ __forceinline__ int case_of_lane(const DevGrid& d, int lane, int ncas
   return d.lane_case ? d.lane_case[lane] : (lane < ncases ? lane : -1);
 }
 
+// A child's contribution block as its parent reads it: offsets of the block and of
+// its right-hand-side part, its size m (= f - w) and the start of its relative map.
+struct ChildRef {
+  long long cb_off, cbr_off;
+  int m, rel_ptr;
+};
+
 struct DevLU {
   int n, nsn, nA;
   long long nnz, sumcb, sumcbr;
@@ -113,6 +120,7 @@ struct DevLU {
   const int* sn_rows;
   const int* child_ptr;
   const int* child_list;
+  const ChildRef* child_ref;  // per child_list position
   const int* sn_parent;
   const int* rel_ptr;
   const int* relmap;
@@ -689,6 +697,13 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
     const int lane = (ch % LPG) * G + lv;  // first of this thread's V lanes
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
+    // the rest of the supernode's description, loaded here with the above (one round
+    // trip) rather than after the barriers of the phases that use it
+    const int ah0 = L.ah_ptr[s], ah1 = L.ah_ptr[s + 1];
+    const int ci0 = L.child_ptr[s], ci1 = L.child_ptr[s + 1];
+    const long long po = L.pan_off[s];
+    const bool has_parent = L.sn_parent[s] >= 0;
+    const long long cbo_s = L.cb_off[s], cbro_s = L.cbr_off[s];
     const int RS = front_stride(f);
     const int ncols = with_rhs ? f + 1 : f;
     // F + (r * RS + c) * G: entry (r, c) of this thread's lanes
@@ -703,8 +718,8 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
     {
       const T* a0 = A + at32(g, L.nA, 0, lane);
       // four entries' index and value loads in flight before their stores
-      const int e1 = L.ah_ptr[s + 1];
-      int e = L.ah_ptr[s] + slot;
+      const int e1 = ah1;
+      int e = ah0 + slot;
       for (; e + 3 * SLOTS < e1; e += 4 * SLOTS) {
         int loc[4];
         LV v[4];
@@ -721,11 +736,14 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
     if (with_rhs)
       for (int p = slot; p < w; p += SLOTS) st<T, V>(FP(p, f), ld<T, V>(x + at32(g, L.n, rows[p], lane)));
     team_sync<TEAM>();
-    for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
-      const int ch2 = L.child_list[ci];
-      const int m = L.sn_f[ch2] - L.sn_w[ch2];
-      const int* rel = L.relmap + L.rel_ptr[ch2];
-      const long long cbo = L.cb_off[ch2];
+    ChildRef next = ci0 < ci1 ? L.child_ref[ci0] : ChildRef{};
+    for (int ci = ci0; ci < ci1; ++ci) {
+      // the next child's reference is loaded while this one is added
+      const ChildRef cr = next;
+      if (ci + 1 < ci1) next = L.child_ref[ci + 1];
+      const int m = cr.m;
+      const int* rel = L.relmap + cr.rel_ptr;
+      const long long cbo = cr.cb_off;
       const int b0 = (m * cg) / CG, b1 = (m * (cg + 1)) / CG;
       for (int a = rs; a < m; a += RSL) {
         T* dst = FP(rel[a], 0);
@@ -760,7 +778,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
         if (with_rhs && cg == 0) {
           T* d = FP(rel[a], f);
           LV o = ld<T, V>(d);
-          const LV v = ld<T, V>(cbr + at32(g, L.sumcbr, L.cbr_off[ch2] + a, lane));
+          const LV v = ld<T, V>(cbr + at32(g, L.sumcbr, cr.cbr_off + a, lane));
 #pragma unroll
           for (int k = 0; k < V; ++k) o.v[k] += v.v[k];
           st<T, V>(d, o);
@@ -843,7 +861,6 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
       team_sync<TEAM>();
     }
     }
-    const long long po = L.pan_off[s];
     T* pbase = pan + at32(g, L.nnz, po, lane);
     // U-panel: rows 0..w-1, all f columns; L-panel: rows w..f-1, columns 0..w-1
     {
@@ -867,15 +884,15 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
     }
     if (with_rhs)
       for (int p = slot; p < w; p += SLOTS) st<T, V>(x + at32(g, L.n, rows[p], lane), ld<T, V>(FP(p, f)));
-    if (L.sn_parent[s] >= 0) {
-      T* cbase = cb + at32(g, L.sumcb, L.cb_off[s], lane);
+    if (has_parent) {
+      T* cbase = cb + at32(g, L.sumcb, cbo_s, lane);
       const int c0 = (m * cg) / CG, c1 = (m * (cg + 1)) / CG;
       for (int a = rs; a < m; a += RSL) {
         T* dst = cbase + (size_t)a * m * 32;
         const T* src = FP(w + a, w);
 #pragma unroll 4
         for (int b = c0; b < c1; ++b) st<T, V>(dst + (size_t)b * 32, ld<T, V>(src + b * G));
-        if (with_rhs && cg == 0) st<T, V>(cbr + at32(g, L.sumcbr, L.cbr_off[s] + a, lane), ld<T, V>(FP(w + a, f)));
+        if (with_rhs && cg == 0) st<T, V>(cbr + at32(g, L.sumcbr, cbro_s + a, lane), ld<T, V>(FP(w + a, f)));
       }
     }
 #undef FP
