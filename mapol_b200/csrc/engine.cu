@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <climits>
 #include <mutex>
 #include <set>
 #include <string>
@@ -91,6 +92,7 @@ constexpr int kFmaxAll = 167;
 
 struct Launch {
   int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
+  int wfmax = 0;                 // largest w * f in range (U-panel entries)
 };
 
 // FNV-1a over the structure that decides the launches and their work
@@ -211,9 +213,12 @@ struct LUSystem {
     level_sched.clear();
     for (int l = 0; l < s.nlevels; ++l) {
       const int b = s.lev_ptr[l], e = s.lev_ptr[l + 1];
-      int fmax_all = 0;
-      for (int k = b; k < e; ++k) fmax_all = std::max(fmax_all, s.sn_f[s.lev_sn[k]]);
-      level_sched.push_back({b, e - b, 0, fmax_all});
+      int fmax_all = 0, wf = 0;
+      for (int k = b; k < e; ++k) {
+        fmax_all = std::max(fmax_all, s.sn_f[s.lev_sn[k]]);
+        wf = std::max(wf, s.sn_w[s.lev_sn[k]] * s.sn_f[s.lev_sn[k]]);
+      }
+      level_sched.push_back({b, e - b, 0, fmax_all, wf});
       int k = b;
       while (k < e) {
         auto cls_of = [](int f) {
@@ -314,6 +319,10 @@ void ensure_attrs(int device) {
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 16, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, 16, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_staged<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_staged<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_staged<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_staged<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G / 2, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
@@ -630,13 +639,36 @@ void tune_factor(LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, 
   tune_cache().factor.emplace(key, best);
 }
 
-// Backward substitution of one level: ge = 0 one case per thread (k_mf_bsolve), else
-// warps over chunks of ge lanes (k_mf_bsolve_chunk).
+// Shared memory of k_mf_bsolve_staged for a level: its largest U panel and front of
+// ge lanes.
+inline size_t bsolve_staged_smem(const Launch& ln, int ge, size_t wsize) {
+  return (size_t)(ln.wfmax + ln.fcap) * ge * wsize;
+}
+
+// Backward substitution of one level: ge = 0 one case per thread (k_mf_bsolve), ge > 0
+// warps over chunks of ge lanes (k_mf_bsolve_chunk), ge < 0 the same with the U panel
+// staged in shared memory first (k_mf_bsolve_staged, chunks of -ge lanes).
 template <typename T>
 void launch_bsolve_one(int ge, const LUSystem& sys, const Launch& ln, int ngroups, const T* pan, T* x,
                        const int* group_active, cudaStream_t st) {
   const DevLU dl = sys.dev();
   const int* ts = sys.lev_sn.as<int>() + ln.offset;
+  if (ge < 0) {
+    // staged U panel: a one-warp block per task
+    const int gs = -ge;
+    const long long ntasks = (long long)ln.count * ngroups * (32 / gs);
+    const unsigned blocks = (unsigned)std::min<long long>(ntasks, 148LL * 32);
+    const size_t smem = bsolve_staged_smem(ln, gs, sizeof(T));
+    switch (gs) {
+      case 8: k_mf_bsolve_staged<T, 8><<<blocks, 32, smem, st>>>(dl, ts, ln.count, ngroups, ln.wfmax, pan, x, group_active); break;
+      case 4: k_mf_bsolve_staged<T, 4><<<blocks, 32, smem, st>>>(dl, ts, ln.count, ngroups, ln.wfmax, pan, x, group_active); break;
+      case 2: k_mf_bsolve_staged<T, 2><<<blocks, 32, smem, st>>>(dl, ts, ln.count, ngroups, ln.wfmax, pan, x, group_active); break;
+      case 1: k_mf_bsolve_staged<T, 1><<<blocks, 32, smem, st>>>(dl, ts, ln.count, ngroups, ln.wfmax, pan, x, group_active); break;
+      default: throw MpfError{MPF_ERR_INTERNAL, "no staged backward-solve kernel for this lane count"};
+    }
+    CUDA_TRY(cudaGetLastError());
+    return;
+  }
   const long long ntasks = (long long)ln.count * ngroups * (ge ? 32 / ge : 1);
   const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
   const size_t smem = (size_t)4 * ln.fcap * (ge ? ge : 32) * sizeof(T);
@@ -666,9 +698,19 @@ template <typename T>
 void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active, cudaStream_t st,
                    int* nlaunch) {
   const auto it = sys.tuned_bs.find({Prec<T>::idx, ngroups});
+  // MPF_BSOLVE_LANES (testing, tuning): every level runs this kernel instead: 0, a lane
+  // count G of k_mf_bsolve_chunk (16, 8, 4, 2, 1), or -G for k_mf_bsolve_staged (8, 4,
+  // 2, 1) on the levels where its shared memory fits
+  int force = INT_MIN;
+  if (const char* e = std::getenv("MPF_BSOLVE_LANES")) {
+    const int v = std::atoi(e);
+    for (int ok : {0, 16, 8, 4, 2, 1, -8, -4, -2, -1})
+      if (v == ok) force = v;
+  }
   for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
     const Launch& ln = sys.level_sched[k];
-    const int ge = it != sys.tuned_bs.end() ? it->second[k] : bsolve_heuristic<T>(ln, ngroups);
+    int ge = it != sys.tuned_bs.end() ? it->second[k] : bsolve_heuristic<T>(ln, ngroups);
+    if (force != INT_MIN && (force >= 0 || bsolve_staged_smem(ln, -force, sizeof(T)) <= kSmemMax)) ge = force;
     launch_bsolve_one<T>(ge, sys, ln, ngroups, pan, x, group_active, st);
     ++*nlaunch;
   }
@@ -707,6 +749,9 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
       std::vector<int> cands{h0};
       for (int ge : {0, 16, 8, 4, 2, 1})
         if (ge != h0) cands.push_back(ge);
+      // staged U panels (negative lane counts) where they fit in shared memory
+      for (int gs : {8, 4, 2, 1})
+        if (bsolve_staged_smem(ln, gs, sizeof(T)) <= kSmemMax) cands.push_back(-gs);
       float bt = 0.0f, ht = 0.0f;
       for (size_t i = 0; i < cands.size(); ++i) {
         launch_bsolve_one<T>(cands[i], sys, ln, ngroups, pan, x, group_active, st);

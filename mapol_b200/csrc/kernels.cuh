@@ -1017,6 +1017,90 @@ __global__ void __launch_bounds__(128) k_mf_bsolve_chunk(DevLU L, const int* __r
   }
 }
 
+// Backward substitution with the U panel staged in shared memory: one warp per
+// (supernode, chunk of G lanes) copies the supernode's whole U panel (w x f entries
+// of its G lanes) and the front's x values into shared memory with asynchronous
+// copies that are all in flight together, then solves row-oriented: SLOTS = 32 / G
+// threads per lane, pivot row r owned by slot r % SLOTS.
+//   1. every pivot row subtracts the columns q >= w (x already known) at once;
+//   2. pivots p = w-1 .. 0: the owner divides row p by U(p,p), and after a warp
+//      barrier every owner subtracts U(r,p) x_p from its rows r < p.
+// Per pivot the dependent chain is one division, one barrier and one multiply-add,
+// instead of a dot product.  Shared memory: (wfmax + fcap) * G values (wfmax =
+// largest w * f of the level).
+template <typename T, int G>
+__global__ void __launch_bounds__(32) k_mf_bsolve_staged(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+                                                         int ngroups, int wfmax, const T* __restrict__ pan,
+                                                         T* __restrict__ x, const int* __restrict__ group_active) {
+  constexpr int SLOTS = 32 / G, LPG = 32 / G;
+  constexpr int V = (int)(16 / sizeof(T)) < G ? (int)(16 / sizeof(T)) : G;  // lanes per copy
+  constexpr int NV = G / V;                                                  // copies per entry
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x & 31;
+  const int slot = tid / G, l = tid % G;
+  T* us = reinterpret_cast<T*>(smem_raw);  // [w * f][G]
+  T* xs = us + (size_t)wfmax * G;          // [f][G]
+  const long long nchunks = (long long)ngroups * LPG;
+  const long long ntasks = (long long)nsn_l * nchunks;
+  for (long long t = blockIdx.x; t < ntasks; t += gridDim.x) {
+    const int s = task_sn[t / nchunks];
+    const int ch = (int)(t % nchunks);
+    const int g = ch / LPG;
+    if (!group_active[g] || !task_here(L, s, g)) continue;
+    const int lane0 = (ch % LPG) * G;
+    const int lane = lane0 + l;
+    const int w = L.sn_w[s], f = L.sn_f[s];
+    const int* rows = L.sn_rows + L.sn_rptr[s];
+    const T* src = pan + at32(g, L.nnz, L.pan_off[s], lane0);
+    const int ncopy = w * f * NV;
+    for (int k = tid; k < ncopy; k += 32) {
+      const int e = k / NV, part = (k % NV) * V;
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(us + (size_t)e * G + part);
+      const T* ga = src + (size_t)e * 32 + part;
+      if constexpr (V * sizeof(T) == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(ga) : "memory");
+      else if constexpr (V * sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(ga) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(ga) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    for (int q = slot; q < f; q += SLOTS) xs[q * G + l] = x[at32(g, L.n, rows[q], lane)];
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncwarp();
+    // 1. the known columns: two rows at a time for independent chains
+    int r = slot;
+    for (; r + SLOTS < w; r += 2 * SLOTS) {
+      const T* u0 = us + (size_t)r * f * G + l;
+      const T* u1 = u0 + (size_t)SLOTS * f * G;
+      T a0 = xs[r * G + l], a1 = xs[(r + SLOTS) * G + l];
+      for (int q = w; q < f; ++q) {
+        const T xq = xs[q * G + l];
+        a0 -= u0[q * G] * xq;
+        a1 -= u1[q * G] * xq;
+      }
+      xs[r * G + l] = a0;
+      xs[(r + SLOTS) * G + l] = a1;
+    }
+    if (r < w) {
+      const T* u0 = us + (size_t)r * f * G + l;
+      T a0 = xs[r * G + l];
+      for (int q = w; q < f; ++q) a0 -= u0[q * G] * xs[q * G + l];
+      xs[r * G + l] = a0;
+    }
+    // 2. the triangle, pivot by pivot (each row is only touched by its owner)
+    for (int p = w - 1; p >= 0; --p) {
+      if (p % SLOTS == slot) xs[p * G + l] /= us[((size_t)p * f + p) * G + l];
+      __syncwarp();
+      const T xp = xs[p * G + l];
+      for (int rr = slot; rr < p; rr += SLOTS) xs[rr * G + l] -= us[((size_t)rr * f + p) * G + l] * xp;
+    }
+    __syncwarp();
+    for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, rows[p], lane)] = xs[p * G + l];
+    __syncwarp();
+  }
+}
+
 // ---------------------------------------------------------------- mismatch of given voltages
 // max |F| per case for voltages given case-major (v[c][i], the layout results use),
 // F = [Re mis_pv; Re mis_pq; Im mis_pq] as newtonpf.h:18-71 (hybrid_checkConvergence,
