@@ -323,15 +323,20 @@ def run_ours(args, rank, world, local_rank):
     value_fp64 = n_cases * world * args.steps / (fp64["ms"] / 1e3)
 
     # roofline of the dominant kernel family of the headline (mixed) solve.
-    # Algorithmic bytes per case per Newton iteration (w = bytes per LU value):
-    #   factor:   2 w nnz(L+U)            solve: w nnz(L+U) + 3*8*n
-    #   mismatch: 16 nb (V) + 16 nb (Sbus) + 8 n (F)     jacobian: 16 nb + w nnz(J)
-    #   update:   8 n + 32 nb
+    # Algorithmic bytes per case per Newton iteration (w = bytes per LU value, the
+    # precision of the Newton system, its solution x and the Jacobian):
+    #   factor:   2 w nnz(L+U) (arrowhead and contribution blocks in, panels out)
+    #   solve:    w nnz(U panels) + 2 w n (the backward substitution reads the pivot rows
+    #             of each supernode and x, and writes x; the forward one is fused into
+    #             the factorisation)
+    #   mismatch: 16 nb (V) + 8 n (F) + w nnz(J) (the Jacobian fill is fused into the
+    #             mismatch pass, so its own family time is 0)
+    #   update:   w n (x) + 32 nb (V read and written)
     def alg_bytes(family, w_lu):
         nb, n, nnz_lu, nnz_j = st["n_bus"], st["n_jac"], st["nnz_lu"], st["nnz_jac"]
-        return {"factor_ms": 2 * w_lu * nnz_lu, "solve_ms": w_lu * nnz_lu + 24 * n,
-                "mismatch_ms": 32 * nb + 8 * n, "jacobian_ms": 16 * nb + w_lu * nnz_j,
-                "update_ms": 8 * n + 32 * nb}.get(family)
+        return {"factor_ms": 2 * w_lu * nnz_lu, "solve_ms": w_lu * st["nnz_lu_upper"] + 2 * w_lu * n,
+                "mismatch_ms": 16 * nb + 8 * n + w_lu * nnz_j, "jacobian_ms": 0,
+                "update_ms": w_lu * n + 32 * nb}.get(family)
 
     fams = {k: v for k, v in mixed["fam"].items() if k != "other_ms"}
     dom = max(fams, key=fams.get)

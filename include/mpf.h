@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define MPF_ABI_VERSION 1
+#define MPF_ABI_VERSION 2
 
 /* algorithms — same values as NR / FDXB / FDBX in src/powerflow/runpf.h:16-18 */
 #define MPF_NR   0
@@ -136,6 +136,9 @@ typedef struct mpf_stats {
   int32_t n_bpp, nnz_bpp_lu, bpp_levels;       /* B'' system */
   int32_t n_cases, case_groups;
   int64_t device_bytes;                        /* device memory held by the handle */
+  int64_t nnz_lu_upper;                        /* entries of the Newton system's U panels (the
+                                                  pivot rows of each supernode: what a backward
+                                                  substitution reads) */
 } mpf_stats;
 
 typedef struct mpf_handle mpf_handle;

@@ -124,4 +124,5 @@ class Stats(ctypes.Structure):
         ("n_cases", ctypes.c_int32),
         ("case_groups", ctypes.c_int32),
         ("device_bytes", ctypes.c_int64),
+        ("nnz_lu_upper", ctypes.c_int64),
     ]

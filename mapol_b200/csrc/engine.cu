@@ -553,36 +553,97 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
   }
 }
 
+inline std::string hex64(uint64_t v) {
+  char b[24];
+  std::snprintf(b, sizeof b, "%llx", (unsigned long long)v);
+  return b;
+}
+// Process-wide tuning results, keyed by (structure fingerprint, precision, groups): every
+// handle of the same grid and batch size in a process runs the same kernels, so their
+// results agree bit for bit (kernels that split a dot product differently round
+// differently).
+//
+// MPF_TUNE_FILE names a text file that carries these results from one process to the
+// next: entries found there are used instead of tuning (each choice is first checked
+// against the launch's candidates; an entry that fails is tuned again), and new
+// results are appended.  Lines:
+//   factor <fingerprint, hex> <precision> <groups> <launches> kind,lanes,tile,teams ...
+//   bsolve <fingerprint, hex> <precision> <groups> <levels> lanes ...
+struct TuneCache {
+  std::mutex mu;
+  bool file_read = false;
+  std::map<std::tuple<uint64_t, int, int>, std::vector<FactorChoice>> factor;
+  std::map<std::tuple<uint64_t, int, int>, std::vector<int>> bsolve;
+};
+// the cache, with the tuning file's entries read on first use (caller holds no lock)
+inline TuneCache& tune_cache() {
+  static TuneCache c;
+  std::lock_guard<std::mutex> lock(c.mu);
+  if (!c.file_read) {
+    c.file_read = true;
+    const char* path = std::getenv("MPF_TUNE_FILE");
+    if (std::FILE* fp = path ? std::fopen(path, "r") : nullptr) {
+      char kind[16];
+      unsigned long long fpr;
+      int prec, ng, n;
+      while (std::fscanf(fp, "%15s %llx %d %d %d", kind, &fpr, &prec, &ng, &n) == 5 && n >= 0 && n <= 1000000) {
+        const auto key = std::make_tuple((uint64_t)fpr, prec, ng);
+        bool ok = true;
+        if (std::strcmp(kind, "factor") == 0) {
+          std::vector<FactorChoice> v(n);
+          for (auto& ch : v) ok = ok && std::fscanf(fp, " %d,%d,%d,%d", &ch.kind, &ch.ge, &ch.tt, &ch.tpb) == 4;
+          if (ok) c.factor[key] = v;
+        } else if (std::strcmp(kind, "bsolve") == 0) {
+          std::vector<int> v(n);
+          for (int& x : v) ok = ok && std::fscanf(fp, " %d", &x) == 1;
+          if (ok) c.bsolve[key] = v;
+        } else {
+          ok = false;
+        }
+        if (!ok) break;
+      }
+      std::fclose(fp);
+    }
+  }
+  return c;
+}
+inline void append_tune_file(const std::string& line) {
+  const char* path = std::getenv("MPF_TUNE_FILE");
+  if (std::FILE* fp = path ? std::fopen(path, "a") : nullptr) {
+    std::fputs(line.c_str(), fp);
+    std::fclose(fp);
+  }
+}
+
 // Autotuner: for each launch, level by level, run every candidate twice (the
 // first run loads the kernel) and keep the one with the shortest second run
 // (CUDA events).  Runs without the right-hand side, so x is not touched; every
 // candidate computes the same panels and contribution blocks, which the next
 // level reads.  Called outside stream capture, once per (precision, groups).
-// Process-wide tuning results, keyed by (structure fingerprint, precision, groups): every
-// handle of the same grid and batch size in a process runs the same kernels, so their
-// results agree bit for bit (kernels that split a dot product differently round
-// differently).
-struct TuneCache {
-  std::mutex mu;
-  std::map<std::tuple<uint64_t, int, int>, std::vector<FactorChoice>> factor;
-  std::map<std::tuple<uint64_t, int, int>, std::vector<int>> bsolve;
-};
-inline TuneCache& tune_cache() {
-  static TuneCache c;
-  return c;
-}
-
 template <typename T>
 void tune_factor(LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, T* x, int* status,
                  const int* group_active, cudaStream_t st) {
   if (sys.tuned.count({Prec<T>::idx, ngroups})) return;
   const auto key = std::make_tuple(sys.fingerprint, Prec<T>::idx, ngroups);
   {
-    std::lock_guard<std::mutex> lock(tune_cache().mu);
-    const auto it = tune_cache().factor.find(key);
-    if (it != tune_cache().factor.end()) {
-      sys.tuned[{Prec<T>::idx, ngroups}] = it->second;
-      return;
+    TuneCache& tc = tune_cache();
+    std::lock_guard<std::mutex> lock(tc.mu);
+    const auto it = tc.factor.find(key);
+    if (it != tc.factor.end()) {
+      // every choice must be one of its launch's candidates (entries may come from a file)
+      bool ok = it->second.size() == sys.factor_sched.size();
+      for (size_t k = 0; ok && k < it->second.size(); ++k) {
+        const FactorChoice& c = it->second[k];
+        bool found = false;
+        for (const FactorChoice& y : factor_candidates<T>(sys.factor_sched[k], ngroups))
+          found = found || (y.kind == c.kind && y.ge == c.ge && y.tt == c.tt && y.tpb == c.tpb);
+        ok = found;
+      }
+      if (ok) {
+        sys.tuned[{Prec<T>::idx, ngroups}] = it->second;
+        return;
+      }
+      tc.factor.erase(it);
     }
   }
   cudaEvent_t e0, e1;
@@ -635,8 +696,14 @@ void tune_factor(LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, T* cbr, 
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   sys.tuned[{Prec<T>::idx, ngroups}] = best;
-  std::lock_guard<std::mutex> lock(tune_cache().mu);
-  tune_cache().factor.emplace(key, best);
+  std::string line = "factor " + hex64(sys.fingerprint) + " " + std::to_string(Prec<T>::idx) + " " +
+                     std::to_string(ngroups) + " " + std::to_string(best.size());
+  for (const FactorChoice& c : best)
+    line += " " + std::to_string(c.kind) + "," + std::to_string(c.ge) + "," + std::to_string(c.tt) + "," +
+            std::to_string(c.tpb);
+  TuneCache& tc = tune_cache();
+  std::lock_guard<std::mutex> lock(tc.mu);
+  if (tc.factor.emplace(key, best).second) append_tune_file(line + "\n");
 }
 
 // Shared memory of k_mf_bsolve_staged for a level: its largest U panel and front of
@@ -725,11 +792,22 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
   if (sys.tuned_bs.count({Prec<T>::idx, ngroups})) return;
   const auto key = std::make_tuple(sys.fingerprint, Prec<T>::idx, ngroups);
   {
-    std::lock_guard<std::mutex> lock(tune_cache().mu);
-    const auto it = tune_cache().bsolve.find(key);
-    if (it != tune_cache().bsolve.end()) {
-      sys.tuned_bs[{Prec<T>::idx, ngroups}] = it->second;
-      return;
+    TuneCache& tc = tune_cache();
+    std::lock_guard<std::mutex> lock(tc.mu);
+    const auto it = tc.bsolve.find(key);
+    if (it != tc.bsolve.end()) {
+      bool ok = it->second.size() == sys.level_sched.size();
+      for (size_t k = 0; ok && k < it->second.size(); ++k) {
+        const int ge = it->second[k];
+        ok = ge == 0 || ge == 16 || ge == 8 || ge == 4 || ge == 2 || ge == 1 ||
+             ((ge == -8 || ge == -4 || ge == -2 || ge == -1) &&
+              bsolve_staged_smem(sys.level_sched[k], -ge, sizeof(T)) <= kSmemMax);
+      }
+      if (ok) {
+        sys.tuned_bs[{Prec<T>::idx, ngroups}] = it->second;
+        return;
+      }
+      tc.bsolve.erase(it);
     }
   }
   const size_t xbytes = (size_t)ngroups * 32 * sys.sym.n * sizeof(T);
@@ -795,8 +873,12 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
   CUDA_TRY(cudaMemcpyAsync(x, saved.p, xbytes, cudaMemcpyDeviceToDevice, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   sys.tuned_bs[{Prec<T>::idx, ngroups}] = best;
-  std::lock_guard<std::mutex> lock(tune_cache().mu);
-  tune_cache().bsolve.emplace(key, best);
+  std::string line = "bsolve " + hex64(sys.fingerprint) + " " + std::to_string(Prec<T>::idx) + " " +
+                     std::to_string(ngroups) + " " + std::to_string(best.size());
+  for (int ge : best) line += " " + std::to_string(ge);
+  TuneCache& tc = tune_cache();
+  std::lock_guard<std::mutex> lock(tc.mu);
+  if (tc.bsolve.emplace(key, best).second) append_tune_file(line + "\n");
 }
 
 template <typename T>
@@ -1652,6 +1734,7 @@ int32_t mpf_get_stats(const mpf_handle* h, mpf_stats* st) {
   st->n_cases = h->ncases;
   st->case_groups = h->ngroups;
   st->device_bytes = (int64_t)h->device_bytes();
+  for (int s = 0; s < g.jac.nsn; ++s) st->nnz_lu_upper += (int64_t)g.jac.sn_w[s] * g.jac.sn_f[s];
   return MPF_OK;
 }
 

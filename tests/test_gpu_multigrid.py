@@ -11,20 +11,16 @@ import pytest
 import mapol_b200 as m
 from oracle import oracle
 
+from .parity import TIGHT_TOL, compare
+
 pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 V_TOL = 1e-8
 
 
-def _compare(res, ref, max_extra_iter=0):
-    conv = res.status == m.runpf.CONVERGED
-    assert np.array_equal(conv, ref["converged"]), np.where(conv != ref["converged"])
-    assert (res.max_mis[conv] < 1e-8).all()
-    d_it = res.iterations[conv] - ref["iterations"][conv]
-    assert (d_it >= 0).all() and (d_it <= max_extra_iter).all(), (res.iterations, ref["iterations"])
-    if conv.any():
-        assert np.abs(res.v[conv] - ref["v"][conv]).max() < V_TOL
+def _compare(res, ref, max_extra_iter=0, tight=None):
+    return compare(res, ref, max_extra_iter, V_TOL, tight)
 
 
 @pytest.fixture(scope="module")
@@ -42,8 +38,10 @@ def test_three_grids_one_batch_match_oracle(cfg2, alg):
         mg.set_cases(cases)
         for prec in (m.FP64, m.MIXED):
             mg.solve(alg, prec)
-            for res, ref in zip(mg.results(), refs):
-                _compare(res, ref, 0 if prec == m.FP64 else 1)
+            for res, ref, (b, br), cs in zip(mg.results(), refs, grids, cases):
+                tight = lambda idx, b=b, br=br, cs=cs: oracle.runpf(b, br, [cs[i] for i in idx], alg=alg,
+                                                                    tol=TIGHT_TOL)
+                _compare(res, ref, 0 if prec == m.FP64 else 1, tight)
 
 
 def test_one_batch_launches_like_its_largest_grid(cfg2):

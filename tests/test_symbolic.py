@@ -28,7 +28,7 @@ def test_library_exports_every_declared_entry_point():
     L = lib()
     missing = [d for d in declared if not hasattr(L, d)]
     assert not missing, missing
-    assert L.mpf_abi_version() == 1
+    assert L.mpf_abi_version() == 2
 
 
 def test_generator_is_deterministic_and_pinned():
