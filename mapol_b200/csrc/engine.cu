@@ -93,6 +93,47 @@ constexpr int kFmaxAll = 167;
 struct Launch {
   int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
   int wfmax = 0;                 // largest w * f in range (U-panel entries)
+  int level = 0;                 // elimination-tree level
+};
+
+// Side streams of one LU system, created on first use.  The factorisation's launches
+// form a DAG (a launch needs the launches that hold its supernodes' children); each task
+// class keeps its launches in order on one stream (class 0 on the caller's), and a
+// launch waits by event only for the latest launch it needs on each other stream, so
+// independent chains (small fronts near the leaves beside large fronts) run side by
+// side; captured in a graph these are parallel branches.
+struct SideStreams {
+  static constexpr int kN = 3;
+  cudaStream_t s[kN] = {};
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> done;  // per factorisation launch
+  SideStreams() = default;
+  SideStreams(const SideStreams&) = delete;
+  SideStreams& operator=(const SideStreams&) = delete;
+  ~SideStreams() {
+    for (int i = 0; i < kN; ++i)
+      if (s[i]) cudaStreamDestroy(s[i]);
+    for (cudaEvent_t e : done) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+  }
+  void ensure(size_t nlaunch) {
+    if (!fork) {
+      for (int i = 0; i < kN; ++i) CUDA_TRY(cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking));
+      CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    }
+    while (done.size() < nlaunch) {
+      cudaEvent_t e;
+      CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      done.push_back(e);
+    }
+  }
+};
+
+// Where each factorisation launch runs and what it waits for (see SideStreams).
+struct LaunchDeps {
+  int stream = 0;                 // 0 = the caller's, 1..3 = side streams
+  std::vector<int> wait;          // launches on other streams to wait for (latest per stream)
+  bool record = false;            // a later launch on another stream waits for this one
 };
 
 // FNV-1a over the structure that decides the launches and their work
@@ -129,6 +170,8 @@ struct LUSystem {
   DevBuf sn_island;                  // multi-island handles only
   const int* group_island = nullptr; // the handle's current per-group islands (or null)
   std::vector<Launch> factor_sched;  // ascending levels
+  std::vector<LaunchDeps> factor_deps;
+  std::unique_ptr<SideStreams> side = std::make_unique<SideStreams>();
   // autotuned kernel of every factor_sched launch, per (precision, case groups)
   uint64_t fingerprint = 0;          // of the symbolic structure (process-wide tuning cache key)
   std::map<std::pair<int, int>, std::vector<FactorChoice>> tuned;
@@ -233,8 +276,32 @@ struct LUSystem {
           fcap = std::max(fcap, f);
           ++k2;
         }
-        factor_sched.push_back({k, k2 - k, cls, fcap});
+        factor_sched.push_back({k, k2 - k, cls, fcap, 0, l});
         k = k2;
+      }
+    }
+    // the launch DAG: streams by task class, waits for the children's launches
+    factor_deps.assign(factor_sched.size(), LaunchDeps{});
+    {
+      std::vector<int> launch_of(s.nsn, -1);
+      for (size_t q = 0; q < factor_sched.size(); ++q) {
+        const Launch& ln = factor_sched[q];
+        factor_deps[q].stream = ln.cls == CLS_S ? 0 : ln.cls == CLS_M1 ? 1 : ln.cls == CLS_M ? 2 : 3;
+        int latest[4] = {-1, -1, -1, -1};
+        for (int t = ln.offset; t < ln.offset + ln.count; ++t) {
+          const int sn = s.lev_sn[t];
+          launch_of[sn] = (int)q;
+          for (int c = s.child_ptr[sn]; c < s.child_ptr[sn + 1]; ++c) {
+            const int j = launch_of[s.child_list[c]];
+            const int js = factor_deps[j].stream;
+            if (js != factor_deps[q].stream) latest[js] = std::max(latest[js], j);
+          }
+        }
+        for (int js = 0; js < 4; ++js)
+          if (latest[js] >= 0) {
+            factor_deps[q].wait.push_back(latest[js]);
+            factor_deps[latest[js]].record = true;
+          }
       }
     }
   }
@@ -545,12 +612,35 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
                    const int* group_active, int with_rhs, cudaStream_t st, int* nlaunch) {
   const auto it = sys.tuned.find({Prec<T>::idx, ngroups});
   const std::vector<FactorChoice>* tuned = it != sys.tuned.end() ? &it->second : nullptr;
-  for (size_t k = 0; k < sys.factor_sched.size(); ++k) {
+  const size_t n = sys.factor_sched.size();
+  auto one = [&](size_t k, cudaStream_t s) {
     const Launch& ln = sys.factor_sched[k];
     const FactorChoice ch = tuned ? (*tuned)[k] : heuristic_choice<T>(ln, ngroups);
-    launch_choice<T>(ch, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+    launch_choice<T>(ch, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, s);
     ++*nlaunch;
+  };
+  // the launch DAG over the caller's stream and three side streams (see SideStreams)
+  SideStreams& ss = *sys.side;
+  ss.ensure(n);
+  cudaStream_t streams[4] = {st, ss.s[0], ss.s[1], ss.s[2]};
+  int last[4] = {-1, -1, -1, -1};  // latest launch on each stream
+  CUDA_TRY(cudaEventRecord(ss.fork, st));
+  bool forked[4] = {true, false, false, false};
+  for (size_t k = 0; k < n; ++k) {
+    const LaunchDeps& dp = sys.factor_deps[k];
+    cudaStream_t s = streams[dp.stream];
+    if (!forked[dp.stream]) {
+      CUDA_TRY(cudaStreamWaitEvent(s, ss.fork, 0));
+      forked[dp.stream] = true;
+    }
+    for (int j : dp.wait) CUDA_TRY(cudaStreamWaitEvent(s, ss.done[j], 0));
+    one(k, s);
+    if (dp.record || dp.stream != 0) CUDA_TRY(cudaEventRecord(ss.done[k], s));
+    last[dp.stream] = (int)k;
   }
+  // join: the caller's stream waits for the last launch of every side stream
+  for (int q = 1; q < 4; ++q)
+    if (last[q] >= 0) CUDA_TRY(cudaStreamWaitEvent(st, ss.done[last[q]], 0));
 }
 
 inline std::string hex64(uint64_t v) {
