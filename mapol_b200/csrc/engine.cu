@@ -171,13 +171,18 @@ struct LUSystem {
   const int* group_island = nullptr; // the handle's current per-group islands (or null)
   std::vector<Launch> factor_sched;  // ascending levels
   std::vector<LaunchDeps> factor_deps;
+  // the backward substitution: the factorisation's launches (one per level and task
+  // class), run from the root down; a launch waits for the launches holding its
+  // supernodes' parents
+  std::vector<Launch> bsolve_sched;
+  std::vector<LaunchDeps> bsolve_deps;
   std::unique_ptr<SideStreams> side = std::make_unique<SideStreams>();
   // autotuned kernel of every factor_sched launch, per (precision, case groups)
   uint64_t fingerprint = 0;          // of the symbolic structure (process-wide tuning cache key)
   std::map<std::pair<int, int>, std::vector<FactorChoice>> tuned;
   // autotuned lane count of every backward-solve level launch (0 = one case per thread)
   std::map<std::pair<int, int>, std::vector<int>> tuned_bs;
-  std::vector<Launch> level_sched;   // one launch per level (solves), ascending
+  std::vector<Launch> level_sched;   // one launch per level (fast-decoupled forward and adjoint solves), ascending
   std::vector<int> ah_host;          // arrowhead ranges (host copy of ah_ptr)
   int nA = 0;
   // values per precision [0] = FP64, [1] = FP32
@@ -278,6 +283,34 @@ struct LUSystem {
         }
         factor_sched.push_back({k, k2 - k, cls, fcap, 0, l});
         k = k2;
+      }
+    }
+    // the backward substitution's launches and their DAG (top-down: parents first)
+    bsolve_sched = factor_sched;
+    for (Launch& ln : bsolve_sched)
+      for (int t = ln.offset; t < ln.offset + ln.count; ++t)
+        ln.wfmax = std::max(ln.wfmax, s.sn_w[s.lev_sn[t]] * s.sn_f[s.lev_sn[t]]);
+    bsolve_deps.assign(bsolve_sched.size(), LaunchDeps{});
+    {
+      std::vector<int> launch_of(s.nsn, -1);
+      for (int q = (int)bsolve_sched.size() - 1; q >= 0; --q) {
+        const Launch& ln = bsolve_sched[q];
+        bsolve_deps[q].stream = ln.cls == CLS_S ? 0 : ln.cls == CLS_M1 ? 1 : ln.cls == CLS_M ? 2 : 3;
+        int latest[4] = {INT_MAX, INT_MAX, INT_MAX, INT_MAX};  // launches run in descending order
+        for (int t = ln.offset; t < ln.offset + ln.count; ++t) {
+          const int sn = s.lev_sn[t];
+          launch_of[sn] = q;
+          const int par = s.sn_parent[sn];
+          if (par < 0) continue;
+          const int j = launch_of[par];
+          const int js = bsolve_deps[j].stream;
+          if (js != bsolve_deps[q].stream) latest[js] = std::min(latest[js], j);
+        }
+        for (int js = 0; js < 4; ++js)
+          if (latest[js] != INT_MAX) {
+            bsolve_deps[q].wait.push_back(latest[js]);
+            bsolve_deps[latest[js]].record = true;
+          }
       }
     }
     // the launch DAG: streams by task class, waits for the children's launches
@@ -864,13 +897,32 @@ void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const i
     for (int ok : {0, 16, 8, 4, 2, 1, -8, -4, -2, -1})
       if (v == ok) force = v;
   }
-  for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
-    const Launch& ln = sys.level_sched[k];
+  // the launch DAG from the root down over the caller's stream and the side streams
+  const int n = (int)sys.bsolve_sched.size();
+  SideStreams& ss = *sys.side;
+  ss.ensure(n);
+  cudaStream_t streams[4] = {st, ss.s[0], ss.s[1], ss.s[2]};
+  int last[4] = {-1, -1, -1, -1};
+  bool forked[4] = {true, false, false, false};
+  CUDA_TRY(cudaEventRecord(ss.fork, st));
+  for (int k = n - 1; k >= 0; --k) {
+    const Launch& ln = sys.bsolve_sched[k];
+    const LaunchDeps& dp = sys.bsolve_deps[k];
+    cudaStream_t s = streams[dp.stream];
+    if (!forked[dp.stream]) {
+      CUDA_TRY(cudaStreamWaitEvent(s, ss.fork, 0));
+      forked[dp.stream] = true;
+    }
+    for (int j : dp.wait) CUDA_TRY(cudaStreamWaitEvent(s, ss.done[j], 0));
     int ge = it != sys.tuned_bs.end() ? it->second[k] : bsolve_heuristic<T>(ln, ngroups);
     if (force != INT_MIN && (force >= 0 || bsolve_staged_smem(ln, -force, sizeof(T)) <= kSmemMax)) ge = force;
-    launch_bsolve_one<T>(ge, sys, ln, ngroups, pan, x, group_active, st);
+    launch_bsolve_one<T>(ge, sys, ln, ngroups, pan, x, group_active, s);
     ++*nlaunch;
+    if (dp.record || dp.stream != 0) CUDA_TRY(cudaEventRecord(ss.done[k], s));
+    last[dp.stream] = k;
   }
+  for (int q = 1; q < 4; ++q)
+    if (last[q] >= 0) CUDA_TRY(cudaStreamWaitEvent(st, ss.done[last[q]], 0));
 }
 
 // Autotuner of the backward solve: per level, each lane count runs twice and the
@@ -886,12 +938,12 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
     std::lock_guard<std::mutex> lock(tc.mu);
     const auto it = tc.bsolve.find(key);
     if (it != tc.bsolve.end()) {
-      bool ok = it->second.size() == sys.level_sched.size();
+      bool ok = it->second.size() == sys.bsolve_sched.size();
       for (size_t k = 0; ok && k < it->second.size(); ++k) {
         const int ge = it->second[k];
         ok = ge == 0 || ge == 16 || ge == 8 || ge == 4 || ge == 2 || ge == 1 ||
              ((ge == -8 || ge == -4 || ge == -2 || ge == -1) &&
-              bsolve_staged_smem(sys.level_sched[k], -ge, sizeof(T)) <= kSmemMax);
+              bsolve_staged_smem(sys.bsolve_sched[k], -ge, sizeof(T)) <= kSmemMax);
       }
       if (ok) {
         sys.tuned_bs[{Prec<T>::idx, ngroups}] = it->second;
@@ -907,12 +959,12 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
   cudaEvent_t e0, e1;
   CUDA_TRY(cudaEventCreate(&e0));
   CUDA_TRY(cudaEventCreate(&e1));
-  std::vector<int> best(sys.level_sched.size(), 0);
+  std::vector<int> best(sys.bsolve_sched.size(), 0);
   const bool log = std::getenv("MPF_TUNE_LOG") != nullptr;
   double sum_best = 0.0, sum_heur = 0.0;
   try {
-    for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
-      const Launch& ln = sys.level_sched[k];
+    for (int k = (int)sys.bsolve_sched.size() - 1; k >= 0; --k) {
+      const Launch& ln = sys.bsolve_sched[k];
       const int h0 = bsolve_heuristic<T>(ln, ngroups);
       std::vector<int> cands{h0};
       for (int ge : {0, 16, 8, 4, 2, 1})
@@ -945,7 +997,7 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
           e += (int64_t)sys.sym.sn_w[sn] * sys.sym.sn_f[sn] + sys.sym.sn_f[sn] + sys.sym.sn_w[sn];
         }
         const double bytes = (double)e * sizeof(T) * 32.0 * ngroups;
-        std::fprintf(stderr, "mpf tune: n %d fp%d groups %d bsolve level %d sn %d fcap %d: heuristic %.1f us, "
+        std::fprintf(stderr, "mpf tune: n %d fp%d groups %d bsolve launch %d sn %d fcap %d: heuristic %.1f us, "
                      "best %.1f us (lanes %d), %.1f MB, %.0f GB/s\n", sys.sym.n, (int)sizeof(T) * 8, ngroups, k,
                      ln.count, ln.fcap, ht * 1e3, bt * 1e3, best[k], bytes * 1e-6, bytes / (bt * 1e-3) * 1e-9);
       }
