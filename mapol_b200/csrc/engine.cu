@@ -158,7 +158,8 @@ inline uint64_t structure_fingerprint(const LUSymbolic& s) {
 // Kernel of one factorisation launch: kind 0 = warp teams (k_mf_factor<T, ge, 32>,
 // tpb teams per block), 1 = 256-thread teams with the LU in shared memory, 2 = the
 // same with the LU in registers (TT x TT tile per thread), 3 = 512- or 1024-thread
-// teams (tpb = threads / 256) with the LU in shared memory
+// teams (tpb = threads / 256) with the LU in shared memory, 5 = 256- or 512-thread teams
+// (tpb = threads / 256) taking two pivots per barrier
 struct FactorChoice {
   int kind, ge, tt, tpb;
 };
@@ -424,6 +425,10 @@ void ensure_attrs(int device) {
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_staged<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_staged<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 256, -2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 512, -2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G / 2, 256, -2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G / 2, 512, -2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G / 2, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor<T, Prec<T>::G / 2, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
@@ -590,11 +595,14 @@ std::vector<FactorChoice> factor_candidates(const Launch& ln, int ngroups) {
   }
   for (int ge = 16; ge >= 1; ge /= 2)
     if (factor_smem_rt(ln.fcap, ge, 1, 0, ws) <= kSmemMax) add({1, ge, 0, 1});
-  // wider teams for large fronts: more threads per pivot step when few tasks run
+  // wider teams for large fronts: more threads per pivot step when few tasks run;
+  // two pivots per barrier
   if (ln.fcap > kFmaxM)
     for (int ge : {G, G / 2})
-      if (factor_smem_rt(ln.fcap, ge, 1, 0, ws) <= kSmemMax)
+      if (factor_smem_rt(ln.fcap, ge, 1, 0, ws) <= kSmemMax) {
         for (int tpb : {2, 4}) add({3, ge, 0, tpb});
+        for (int tpb : {1, 2}) add({5, ge, 0, tpb});
+      }
   const int tt = reg_tt(ln.fcap);
   if (ln.fcap > kFmaxS && tt <= kRegTTMax)
     for (int ge = reg_lanes_max<T>(tt); ge >= 1; ge /= 2)
@@ -625,6 +633,20 @@ void launch_choice(const FactorChoice& ch, const LUSystem& sys, const Launch& ln
       launch_factor_ge<T>(ch.ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
   } else if (ch.kind == 2) {
     launch_factor_reg<T>(ch.ge, ch.tt, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+  } else if (ch.kind == 5) {
+    const bool wide = ch.tpb == 2;
+    if (ch.ge == G && wide)
+      launch_factor_one<T, G, 512, -2>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+    else if (ch.ge == G)
+      launch_factor_one<T, G, 256, -2>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st, 1);
+    else if (ch.ge == G / 2 && wide)
+      launch_factor_one<T, G / 2, 512, -2>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st,
+                                           1);
+    else if (ch.ge == G / 2)
+      launch_factor_one<T, G / 2, 256, -2>(sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st,
+                                           1);
+    else
+      throw MpfError{MPF_ERR_INTERNAL, "no two-pivot kernel for this lane count"};
   } else {
     const bool big = ch.tpb == 4;
     if (ch.ge == G && big)

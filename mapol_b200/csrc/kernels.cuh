@@ -663,9 +663,10 @@ __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int
 }
 
 // TT > 0: the partial LU runs in registers (lu_registers; TEAM 256 with one thread
-// per entry-lane group, i.e. G <= 16 bytes of lanes); TT = 0: in shared memory.
+// per entry-lane group, i.e. G <= 16 bytes of lanes); TT = 0: in shared memory, one
+// barrier per pivot; TT = -2: in shared memory, two pivots per barrier.
 template <typename T, int G, int TEAM, int TT = 0>
-__global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 256 ? 1 : 4)) k_mf_factor(
+__global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 256 ? 1 : (TT < 0 ? 2 : 4))) k_mf_factor(
     DevLU L, const int* __restrict__ task_sn, int nsn_l, int ngroups, int fcap,
     const T* __restrict__ A, T* __restrict__ pan, T* __restrict__ cb, T* __restrict__ cbr,
     T* __restrict__ x, int* __restrict__ status, const int* __restrict__ group_active, int with_rhs) {
@@ -791,6 +792,160 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
       T* bufs = reinterpret_cast<T*>(smem_raw) + (size_t)fcap * front_stride(fcap) * G;
       lu_registers<T, V, TT>(F, RS, f, ncols, w, bufs, bufs + 2 * (size_t)fcap * G, fcap, status + g * 32 + lane,
                              tid == 0);
+    } else if constexpr (TT < 0) {
+    // Right-looking partial LU, two pivots (p, p1 = p + 1) per team barrier.  Every
+    // thread computes both pivots' inverses, u = F(p,p1) and l = F(p1,p) / F(p,p); rows
+    // i > p1 then take both rank-1 updates at once on columns q > p1:
+    //   l0 = F(i,p) / F(p,p);  x1 = F(i,p1) - l0 u;  l1 = x1 / F'(p1,p1)
+    //   F(i,q) = (F(i,q) - l0 F(p,q)) - l1 (F(p1,q) - l F(p,q))
+    // Row p1 (updated by pivot p) and columns p, p1 (scaled, and column p1 updated by
+    // pivot p) are read by every thread during the step, so they are written at the
+    // start of the next step (no thread reads them there) or after the last one.
+    // Every entry sees the operations of the one-pivot loop in the same order, so the
+    // factors are the same bit for bit.
+    auto pivot_inverse = [&](LV piv) {
+      LV inv;
+#pragma unroll
+      for (int k = 0; k < V; ++k) {
+        T pk = piv.v[k];
+        if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
+          if (slot == 0) status[g * 32 + lane + k] = ST_SINGULAR;
+          pk = (T)1;
+        }
+        inv.v[k] = (T)1 / pk;
+      }
+      return inv;
+    };
+    int pend = 0, pc = 0;  // deferred work of the last step: 1 = one pivot pc, 2 = pivots pc, pc + 1
+    LV pinv0, pinv1, pu, pl;
+    auto finish = [&]() {
+      if (pend == 1) {
+        for (int i = pc + 1 + slot; i < f; i += SLOTS) {
+          LV c = ld<T, V>(FP(i, pc));
+#pragma unroll
+          for (int k = 0; k < V; ++k) c.v[k] *= pinv0.v[k];
+          st<T, V>(FP(i, pc), c);
+        }
+      } else if (pend == 2) {
+        const int p1 = pc + 1;
+        for (int i = p1 + slot; i < f; i += SLOTS) {
+          LV c0 = ld<T, V>(FP(i, pc));
+#pragma unroll
+          for (int k = 0; k < V; ++k) c0.v[k] *= pinv0.v[k];
+          st<T, V>(FP(i, pc), c0);
+          if (i > p1) {
+            LV c1 = ld<T, V>(FP(i, p1));
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+              c1.v[k] = c1.v[k] - c0.v[k] * pu.v[k];
+              c1.v[k] *= pinv1.v[k];
+            }
+            st<T, V>(FP(i, p1), c1);
+          }
+        }
+        for (int q = p1 + slot; q < ncols; q += SLOTS) {
+          LV r1 = ld<T, V>(FP(p1, q));
+          const LV r0 = ld<T, V>(FP(pc, q));
+#pragma unroll
+          for (int k = 0; k < V; ++k) r1.v[k] = r1.v[k] - pl.v[k] * r0.v[k];
+          st<T, V>(FP(p1, q), r1);
+        }
+      }
+      pend = 0;
+    };
+    for (int p = 0; p < w;) {
+      const LV inv0 = pivot_inverse(ld<T, V>(FP(p, p)));
+      if (p + 1 < w) {
+        const int p1 = p + 1;
+        const LV u = ld<T, V>(FP(p, p1));
+        LV l = ld<T, V>(FP(p1, p)), piv1 = ld<T, V>(FP(p1, p1));
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+          l.v[k] *= inv0.v[k];
+          piv1.v[k] = piv1.v[k] - l.v[k] * u.v[k];
+        }
+        const LV inv1 = pivot_inverse(piv1);
+        finish();
+        const int nq = ncols - (p1 + 1);
+        const int q0 = p1 + 1 + (nq * cg) / CG, q1 = p1 + 1 + (nq * (cg + 1)) / CG;
+        const T* rp0 = FP(p, 0);
+        const T* rp1 = FP(p1, 0);
+        for (int i = p1 + 1 + rs; i < f; i += RSL) {
+          T* ri = FP(i, 0);
+          const LV a0 = ld<T, V>(ri + p * G), a1 = ld<T, V>(ri + p1 * G);
+          LV l0, l1;
+#pragma unroll
+          for (int k = 0; k < V; ++k) {
+            l0.v[k] = a0.v[k] * inv0.v[k];
+            const T x1 = a1.v[k] - l0.v[k] * u.v[k];
+            l1.v[k] = x1 * inv1.v[k];
+          }
+          int q = q0;
+          for (; q + 2 <= q1; q += 2) {
+            LV r0[2], r1[2], b[2];
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+              r0[t] = ld<T, V>(rp0 + (q + t) * G);
+              r1[t] = ld<T, V>(rp1 + (q + t) * G);
+              b[t] = ld<T, V>(ri + (q + t) * G);
+            }
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+#pragma unroll
+              for (int k = 0; k < V; ++k) {
+                const T u1 = r1[t].v[k] - l.v[k] * r0[t].v[k];
+                b[t].v[k] = b[t].v[k] - l0.v[k] * r0[t].v[k];
+                b[t].v[k] = b[t].v[k] - l1.v[k] * u1;
+              }
+              st<T, V>(ri + (q + t) * G, b[t]);
+            }
+          }
+          for (; q < q1; ++q) {
+            const LV r0 = ld<T, V>(rp0 + q * G), r1 = ld<T, V>(rp1 + q * G);
+            LV b = ld<T, V>(ri + q * G);
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+              const T u1 = r1.v[k] - l.v[k] * r0.v[k];
+              b.v[k] = b.v[k] - l0.v[k] * r0.v[k];
+              b.v[k] = b.v[k] - l1.v[k] * u1;
+            }
+            st<T, V>(ri + q * G, b);
+          }
+        }
+        pend = 2;
+        pc = p;
+        pinv0 = inv0;
+        pinv1 = inv1;
+        pu = u;
+        pl = l;
+        p += 2;
+      } else {
+        finish();
+        const int nq = ncols - (p + 1);
+        const int q0 = p + 1 + (nq * cg) / CG, q1 = p + 1 + (nq * (cg + 1)) / CG;
+        const T* rp = FP(p, 0);
+        for (int i = p + 1 + rs; i < f; i += RSL) {
+          T* ri = FP(i, 0);
+          LV lip = ld<T, V>(ri + p * G);
+#pragma unroll
+          for (int k = 0; k < V; ++k) lip.v[k] *= inv0.v[k];
+          for (int q = q0; q < q1; ++q) {
+            const LV a = ld<T, V>(rp + q * G);
+            LV b = ld<T, V>(ri + q * G);
+#pragma unroll
+            for (int k = 0; k < V; ++k) b.v[k] = b.v[k] - lip.v[k] * a.v[k];
+            st<T, V>(ri + q * G, b);
+          }
+        }
+        pend = 1;
+        pc = p;
+        pinv0 = inv0;
+        p += 1;
+      }
+      team_sync<TEAM>();
+    }
+    finish();
+    team_sync<TEAM>();
     } else {
     // Right-looking partial LU of the w pivots, one team barrier per pivot.  At
     // pivot p every thread reads the unscaled column p (l_ip = F(i,p) / F(p,p));
