@@ -81,7 +81,9 @@ struct LUSymbolic {
 // Measured on the 9241-bus workload (1000 N-1 cases, mixed precision, solves/s):
 // none 20.5k, zero-free merges only 21.3k, (4, 0.1) 21.9k, (16, 0.3) 20.4k,
 // (32, 0.4) 18.3k, (64, 0.5) 16.7k: the kernels' per-task cost is now low enough
-// that explicit zeros cost more than the tasks they save.
+// that explicit zeros cost more than the tasks they save.  Again with the launch DAG
+// and the two-pivot kernels: these defaults 29.7k; zeros (8, 0.15) 28.9k, (2, 0.05)
+// 29.0k; 48 pivots / 100 rows 29.7k; 16 pivots 29.6k.
 struct Relax {
   int max_pivots = 32;
   int max_front = 83;
