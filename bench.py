@@ -169,20 +169,54 @@ def cpu_port_baseline(buses, branches, cases, budget_s=15.0):
         r = oracle.runpf(buses, branches, cases[:n2], alg=0, solver=oracle.SOLVER_GP, threads=threads)
         dt = time.perf_counter() - t
         n = n2
-    return {"value": n / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+    line = {"value": n / dt, "unit": "solves/s", "cores": threads, "kind": "port",
             "sample": f"{n} of the {len(cases)} N-1 cases, NR FP64 to 1e-8, oracle sparse LU "
                       f"(Gilbert-Peierls, minimum degree), {threads} threads, {dt:.1f} s",
             "converged": int(r["converged"].sum())}
+    return line, r
+
+
+def accuracy(res, ref):
+    """Per-result accuracy of GPU results against the FP64 oracle on the cases both
+    solved: max |dV| (p.u., complex difference), max angle error (degrees), flag and
+    iteration-count mismatches (iterations: mixed precision may take one more)."""
+    n = len(ref["converged"])
+    conv_g = res.status[:n] == 1
+    conv_o = ref["converged"]
+    both = conv_g & conv_o
+    dv = np.abs(res.v[:n][both] - ref["v"][both])
+    dang = np.abs(np.angle(res.v[:n][both] * np.conj(ref["v"][both]), deg=True))
+    d_it = res.iterations[:n] - ref["iterations"]
+    return {"n_compared": int(n), "max_dv": float(dv.max()) if dv.size else None,
+            "max_dangle_deg": float(dang.max()) if dang.size else None,
+            "flag_mismatches": int((conv_g != conv_o).sum()),
+            "iter_equal": int((d_it[both] == 0).sum()), "iter_plus_one": int((d_it[both] == 1).sum()),
+            "iter_other": int(((d_it[both] != 0) & (d_it[both] != 1)).sum())}
+
+
+METRIC = "N-1 PF solves/sec @1e-8 pu, 9241-bus synth: mixed vs plain FP64; HBM GB/s"
+
+
+def fixture_workload(name):
+    """(buses, branches, cases) of a workload from its committed fixture (numpy only:
+    the CPU arms must not load libmpf.so)."""
+    path = os.path.join(ROOT, "tests", "golden", f"workload_{name}.npz")
+    if not os.path.exists(path):
+        return None
+    g = np.load(path)
+    return g["buses"], g["branches"], [[int(b)] for b in g["outages"]]
 
 
 def reference_arm(args):
     """Reference's own CPU path on this host: the NR of mkl_newtonpf with the
     reference's Eigen SparseLU option (newtonpf.h:341-363, compute() every solve),
     from the oracle build compiled against the reference's vendored Eigen."""
-    import mapol_b200 as m
     from oracle import oracle
 
-    buses, branches, cases = m.workload(args.workload)
+    wl = fixture_workload(args.workload)
+    if wl is None:
+        return {"impl": "reference", "unavailable": f"no committed fixture for workload {args.workload}"}
+    buses, branches, cases = wl
     if not oracle.has_eigen():
         return {"impl": "reference", "unavailable": "oracle/_ref (reference Eigen build) not present"}
     threads = os.cpu_count() or 1
@@ -203,7 +237,7 @@ def reference_arm(args):
     per_step = sum(times) / len(times)
     value = len(sample) / (iters * per_step)
     return {
-        "impl": "reference", "metric": "N-1 PF solves/sec @1e-8 pu, 9241-bus synth", "value": value,
+        "impl": "reference", "metric": METRIC, "value": value,
         "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded generator)",
@@ -233,7 +267,9 @@ def run_ours(args, rank, world, local_rank):
     if args.cases:
         cases = cases[: args.cases]
     n_cases = len(cases)
+    t_create = time.perf_counter()
     pf = m.PowerFlow(buses, branches, device=local_rank)
+    t_create = time.perf_counter() - t_create
     pf.set_cases(cases)
     stream = torch.cuda.current_stream()
 
@@ -272,7 +308,7 @@ def run_ours(args, rank, world, local_rank):
         res = pf.results()
         conv = res.status == T.CASE_CONVERGED
         iters_sum = int(res.iterations[conv].sum())
-        out[name] = dict(ms=ms, fam={k: v / args.steps for k, v in fam.items()}, launches=launches,
+        out[name] = dict(res=res, ms=ms, fam={k: v / args.steps for k, v in fam.items()}, launches=launches,
                          n_conv=int(conv.sum()), iters=np.bincount(res.iterations, minlength=11).tolist(),
                          max_mis=float(res.max_mis[conv].max()) if conv.any() else None,
                          iters_sum=iters_sum, nfact=nfact / args.steps)
@@ -352,7 +388,7 @@ def run_ours(args, rank, world, local_rank):
                                             "GB/s": round(b * units / (v / 1e3) / 1e9, 1) if v > 0 else None}
 
     line = {
-        "metric": "N-1 PF solves/sec @1e-8 pu, 9241-bus synth: mixed vs plain FP64; HBM GB/s",
+        "metric": METRIC,
         "value": value,
         "unit": "solves/s",
         "n_gpus": world,
@@ -385,8 +421,13 @@ def run_ours(args, rank, world, local_rank):
     }
     if e2e:
         line["e2e"] = e2e
+    line["setup"] = {"mpf_create_ms": round(t_create * 1e3, 1),
+                     "note": "one-time host symbolic analysis (ordering, supernodes, relative maps) and "
+                             "upload of the shared arrays; not inside the timed solves"}
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_port_baseline(buses, branches, cases)
+        line["cpu_baseline"], ref = cpu_port_baseline(buses, branches, cases)
+        line["accuracy"] = {"vs": "FP64 CPU oracle on the cpu_baseline sample",
+                            "mixed": accuracy(mixed["res"], ref), "fp64": accuracy(fp64["res"], ref)}
     return line
 
 

@@ -268,16 +268,20 @@ int32_t mpf_runpf_host(mpf_handle* h, int32_t alg, int32_t precision,
 int32_t mpf_mismatch(mpf_handle* h, const double* v, double* max_mis, void* stream);
 
 /* Same result as mpf_mismatch, for callers that must not allocate device memory at
- * this point: code running inside CUDA stream capture, real-time loops that may not
- * enter an allocator, or processes where another framework's memory pool owns the
- * GPU.  No counterpart in the reference.  The call allocates nothing: its
- * accumulator is a fixed 512 KB device array built into the library (held on every
- * GPU that loads it until the process exits), so a batch may have at most 65536
- * cases (MPF_ERR_BAD_INPUT beyond that).  The handle itself (mpf_create,
- * mpf_set_cases) must have been set up beforehand.  The first call on each device
- * looks up the array's device address; make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (different
- * streams, or different handles on the same device) race and must be serialised. */
+ * this point: real-time control loops that may not enter an allocator (cudaMalloc can
+ * block and synchronise the device), or processes where another framework's caching
+ * pool owns the GPU's memory, so a fresh cudaMalloc may fail or fragment it.  No
+ * counterpart in the reference.  The call allocates nothing: its accumulator is a
+ * fixed 512 KB device array built into the library (held on every GPU that loads it
+ * until the process exits), so a batch may have at most 65536 cases
+ * (MPF_ERR_BAD_INPUT beyond that).  The handle itself (mpf_create, mpf_set_cases)
+ * must have been set up beforehand.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress) and keeps it for the life of the
+ * process; make that first call before any stream capture, and reload the library
+ * after a cudaDeviceReset, which invalidates the kept address.  All calls share the
+ * array and each clears its own slots first: calls that overlap on the GPU
+ * (different streams, or different handles on the same device) race and must be
+ * serialised. */
 int32_t mpf_mismatch_noalloc(mpf_handle* h, const double* v, double* max_mis, void* stream);
 
 /* Branch ratings (host array [n_branch], p.u. of apparent power; NULL clears them),

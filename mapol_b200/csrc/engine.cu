@@ -2400,7 +2400,7 @@ int32_t mpf_mismatch(mpf_handle* h, const double* v, double* max_mis, void* stre
       CUDA_TRY(cudaMemset(h->eval_acc.p, 0, need));
     }
     const int nfree = (int)h->g.mis_rows.size();
-    k_mismatch_eval<<<dim3((unsigned)((nfree + 255) / 256), (unsigned)h->ncases), 256, 0, st>>>(
+    k_mismatch_eval<<<dim3((unsigned)((nfree + 255) / 256), (unsigned)std::min(h->ncases, 65535)), 256, 0, st>>>(
         h->dev(), reinterpret_cast<const double2*>(v), h->ncases, h->eval_acc.as<unsigned long long>());
     CUDA_TRY(cudaGetLastError());
     k_acc_drain<<<(h->ncases + 255) / 256, 256, 0, st>>>(h->eval_acc.as<unsigned long long>(), max_mis, h->ncases);
@@ -2427,11 +2427,12 @@ int32_t mpf_mismatch_noalloc(mpf_handle* h, const double* v, double* max_mis, vo
     // the array keeps whatever the previous call left: clear this call's slots
     CUDA_TRY(cudaMemsetAsync(acc, 0, (size_t)h->ncases * sizeof(unsigned long long), st));
     const int nfree = (int)h->g.mis_rows.size();
-    k_mismatch_eval<<<dim3((unsigned)((nfree + 255) / 256), (unsigned)h->ncases), 256, 0, st>>>(
+    k_mismatch_eval<<<dim3((unsigned)((nfree + 255) / 256), (unsigned)std::min(h->ncases, 65535)), 256, 0, st>>>(
         h->dev(), reinterpret_cast<const double2*>(v), h->ncases, acc);
     CUDA_TRY(cudaGetLastError());
     k_acc_drain<<<(h->ncases + 255) / 256, 256, 0, st>>>(acc, max_mis, h->ncases);
     CUDA_TRY(cudaGetLastError());
+    h->last_stream = st;  // later set_cases / set_controls wait for these reads
     return MPF_OK;
   });
 }

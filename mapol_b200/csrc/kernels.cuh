@@ -1264,41 +1264,42 @@ __global__ void __launch_bounds__(32) k_mf_bsolve_staged(DevLU L, const int* __r
 // folds them with shuffles, then one atomicMax per warp into acc[c].
 __global__ void __launch_bounds__(256) k_mismatch_eval(DevGrid d, const double2* __restrict__ v, int ncases,
                                                        unsigned long long* __restrict__ acc) {
-  const int c = blockIdx.y;  // the user's case; its lane is ln
-  if (c >= ncases) return;
-  const int ln = lane_of_case(d, c);
-  LaneOut o;
-  load_outages(d, ln, o);
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double m = 0.0;
-  if (r < d.nfree && row_here(d, d.mis_rows[r], ln >> 5)) {
-    const double2* vc = v + (size_t)c * d.nb;
-    const int i = d.mis_rows[r];
-    double2 ib = make_double2(0.0, 0.0);
-    const bool touched = row_touched(o, d.y_diag[i]);
-    for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
-      const double2 y = yentry(d, o, touched, p, ln >> 5, ln & 31);
-      const double2 vj = vc[d.y_col[p]];
-      ib.x += y.x * vj.x - y.y * vj.y;
-      ib.y += y.x * vj.y + y.y * vj.x;
+  // cases stride over gridDim.y (at most 65535), so any batch size launches
+  for (int c = blockIdx.y; c < ncases; c += gridDim.y) {  // the user's case; its lane is ln
+    const int ln = lane_of_case(d, c);
+    LaneOut o;
+    load_outages(d, ln, o);
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0;
+    if (r < d.nfree && row_here(d, d.mis_rows[r], ln >> 5)) {
+      const double2* vc = v + (size_t)c * d.nb;
+      const int i = d.mis_rows[r];
+      double2 ib = make_double2(0.0, 0.0);
+      const bool touched = row_touched(o, d.y_diag[i]);
+      for (int p = d.y_rowptr[i]; p < d.y_rowptr[i + 1]; ++p) {
+        const double2 y = yentry(d, o, touched, p, ln >> 5, ln & 31);
+        const double2 vj = vc[d.y_col[p]];
+        ib.x += y.x * vj.x - y.y * vj.y;
+        ib.y += y.x * vj.y + y.y * vj.x;
+      }
+      const double2 vi = vc[i];
+      double2 s = d.sbus_case ? d.sbus_case[at32(ln >> 5, d.nb, i, ln & 31)] : d.sbus0[i];
+      const bool pvi = still_pv(d, i, ln >> 5, ln & 31);
+      if (d.sw_index && !pvi && d.sw_index[i] >= 0) s.y = d.q_fix[at32(ln >> 5, d.nsw, d.sw_index[i], ln & 31)];
+      const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
+      const double mi = vi.y * ib.x - vi.x * ib.y - s.y;
+      m = fabs(mr);
+      if (mr != mr) m = INFINITY;
+      if (d.jvar[i].y >= 0 && !pvi) {
+        m = fmax(m, fabs(mi));
+        if (mi != mi) m = INFINITY;
+      }
+      m = finite_or_inf(m);
     }
-    const double2 vi = vc[i];
-    double2 s = d.sbus_case ? d.sbus_case[at32(ln >> 5, d.nb, i, ln & 31)] : d.sbus0[i];
-    const bool pvi = still_pv(d, i, ln >> 5, ln & 31);
-    if (d.sw_index && !pvi && d.sw_index[i] >= 0) s.y = d.q_fix[at32(ln >> 5, d.nsw, d.sw_index[i], ln & 31)];
-    const double mr = vi.x * ib.x + vi.y * ib.y - s.x;
-    const double mi = vi.y * ib.x - vi.x * ib.y - s.y;
-    m = fabs(mr);
-    if (mr != mr) m = INFINITY;
-    if (d.jvar[i].y >= 0 && !pvi) {
-      m = fmax(m, fabs(mi));
-      if (mi != mi) m = INFINITY;
-    }
-    m = finite_or_inf(m);
-  }
 #pragma unroll
-  for (int k = 16; k > 0; k >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, k));
-  if ((threadIdx.x & 31) == 0) atomicMax(&acc[c], (unsigned long long)__double_as_longlong(m));
+    for (int k = 16; k > 0; k >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, k));
+    if ((threadIdx.x & 31) == 0) atomicMax(&acc[c], (unsigned long long)__double_as_longlong(m));
+  }
 }
 
 // acc (bits of non-negative doubles) -> out, and acc back to zero for the next call

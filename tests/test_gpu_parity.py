@@ -56,7 +56,7 @@ def test_fd_fp64_matches_oracle(gpu, name, alg):
         pf.set_cases(cases)
         pf.solve(alg, m.FP64)
         res = pf.results()
-    _compare(res, ref, v_tol=1e-7)
+    _compare(res, ref)  # measured: |V - V_oracle| <= 2.4e-13 on these workloads
 
 
 @pytest.mark.parametrize("name", ["cfg0_30bus", "cfg1_300bus"])
@@ -147,27 +147,23 @@ def test_bad_inputs_raise_not_crash(gpu):
         m.PowerFlow(bad, branches)
 
 
-def test_full_size_9241_bus_sample_matches_oracle(gpu):
-    """The 9241-bus workload (all 1000 cases solved on the GPU), with 48 of them
-    checked against the oracle and every case checked by its own mismatch."""
+def test_full_size_9241_bus_all_cases_match_oracle(gpu):
+    """The headline workload at full size: all 1000 N-1 cases of the 9241-bus grid,
+    in both precisions, against the oracle on every case.  Flags identical, FP64
+    iteration counts identical (mixed at most one more), |V - V_oracle| < 1e-8 p.u.
+    (a mixed case that took the extra iteration against the oracle run to 1e-11)."""
     buses, branches, cases = m.workload("cfg3_9241bus")
+    assert len(cases) == 1000
     with m.PowerFlow(buses, branches) as pf:
         pf.set_cases(cases)
         pf.solve(m.NR, m.FP64)
         res = pf.results()
         pf.solve(m.NR, m.MIXED)
         res_mixed = pf.results()
-    conv = res.status == m.runpf.CONVERGED
-    assert conv.mean() > 0.95
-    assert (res.max_mis[conv] < 1e-8).all()
-    conv_m = res_mixed.status == m.runpf.CONVERGED
-    assert np.array_equal(conv, conv_m)
-    assert (res_mixed.iterations[conv] <= res.iterations[conv] + 1).all()
-    assert np.abs(res_mixed.v[conv] - res.v[conv]).max() < 1e-7
-    idx = np.linspace(0, len(cases) - 1, 48).astype(int)
-    ref = _oracle(buses, branches, [cases[i] for i in idx], m.NR)
-    sub = type(res)(res.v[idx], res.iterations[idx], res.status[idx], res.max_mis[idx])
-    _compare(sub, ref)
+    ref = _oracle(buses, branches, cases, m.NR)
+    conv = _compare(res, ref)
+    _compare(res_mixed, ref, max_extra_iter=1, tight=_tight(buses, branches, cases, m.NR))
+    assert conv.all()  # every case of this workload has a solution (non-bridge outages)
 
 
 def test_mismatch_entry_point_matches_solve_and_oracle(gpu):
