@@ -8,8 +8,9 @@ convergence.  ours: prints one JSON line (rank 0) with value = mixed-precision
 solves/s (all ranks), plain FP64 beside it, per-kernel roofline of the dominant
 kernel, the end-to-end figure through the host C-ABI call, the CPU baseline and
 the GPU clocks seen during the timed region.  reference: times the reference's
-own CPU implementation of the path (its Eigen SparseLU option, the oracle build
-compiled against the reference's vendored Eigen) on this host's cores.
+own CPU implementation of the path (mkl_runpf / mkl_newtonpf with its Eigen SparseLU
+option, compiled from the reference's sources into oracle/_ref/librefpf.so) on this
+host's cores.
 
 Multi-GPU: one process per GPU (torchrun); each rank solves its own 1000-case
 N-1 set of the same grid (weak scaling, no data-path collective); the time is
@@ -197,55 +198,115 @@ def accuracy(res, ref):
 METRIC = "N-1 PF solves/sec @1e-8 pu, 9241-bus synth: mixed vs plain FP64; HBM GB/s"
 
 
-def fixture_workload(name):
-    """(buses, branches, cases) of a workload from its committed fixture (numpy only:
-    the CPU arms must not load libmpf.so)."""
-    path = os.path.join(ROOT, "tests", "golden", f"workload_{name}.npz")
-    if not os.path.exists(path):
-        return None
-    g = np.load(path)
-    return g["buses"], g["branches"], [[int(b)] for b in g["outages"]]
+def _ref_worker(conn, fixture, case_ids, solver):
+    """One host core running the reference's own Newton-Raphson (oracle/_ref/librefpf.so,
+    one grid per process: the reference keeps its state in globals).  Each "step"
+    command runs one Newton iteration of its current case (starting the next case of
+    its share when the last one finished) and answers (seconds, iterations done,
+    solves finished, their total iterations, converged count)."""
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    from oracle import refpf
+
+    g = np.load(fixture)
+    outs = g["outages"]
+    st = refpf.Stepper(g["buses"], g["branches"], solver)
+    k = 0
+    conn.send("ready")
+    while conn.recv() == "step":
+        t = time.perf_counter()
+        r = st.step([int(outs[case_ids[k % len(case_ids)]])])
+        dt = time.perf_counter() - t
+        done = (1, r[1], int(r[0])) if r is not None else (0, 0, 0)
+        if r is not None:
+            k += 1
+        conn.send((dt, 1, *done))
+    st.close()
+    conn.close()
 
 
 def reference_arm(args):
-    """Reference's own CPU path on this host: the NR of mkl_newtonpf with the
-    reference's Eigen SparseLU option (newtonpf.h:341-363, compute() every solve),
-    from the oracle build compiled against the reference's vendored Eigen."""
-    from oracle import oracle
+    """The reference's own CPU path on this host's cores: mkl_runpf / mkl_newtonpf
+    (runpf.h:259-352, newtonpf.h:365-523) with its Eigen_SparseLU solver option
+    (newtonpf.h:341-363), compiled unmodified from the reference tree into
+    oracle/_ref/librefpf.so (MKL routines through the in-project stand-in of
+    oracle/refshim/mkl.h).  One process per host core (the reference's state is
+    global); a step is one Newton iteration on every core (a 9241-bus iteration takes
+    seconds), each core walking through its share of the 1000 N-1 cases; solves/s =
+    Newton iterations per second / iterations per solve, both counted from the
+    reference's own solves during the run."""
+    import multiprocessing as mp
 
-    wl = fixture_workload(args.workload)
-    if wl is None:
+    from oracle import refpf
+
+    fixture = os.path.join(ROOT, "tests", "golden", f"workload_{args.workload}.npz")
+    if not os.path.exists(fixture):
         return {"impl": "reference", "unavailable": f"no committed fixture for workload {args.workload}"}
-    buses, branches, cases = wl
-    if not oracle.has_eigen():
-        return {"impl": "reference", "unavailable": "oracle/_ref (reference Eigen build) not present"}
-    threads = os.cpu_count() or 1
-    sample = cases[:threads]
-    # iterations each case needs (own solver, same arithmetic path apart from the LU)
-    it_ref = oracle.runpf(buses, branches, sample, alg=0, solver=oracle.SOLVER_GP, threads=threads)["iterations"]
-    iters = float(np.mean(it_ref))
+    if not refpf.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/librefpf.so (the reference's CPU path built from "
+                                                    "its sources) is not present"}
+    n_cases = len(np.load(fixture)["outages"])
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    conns, procs = [], []
+    for w in range(cores):
+        a, b = ctx.Pipe()
+        p = ctx.Process(target=_ref_worker, args=(b, fixture, list(range(w, n_cases, cores)), refpf.SOLVER_EIGEN))
+        p.start()
+        conns.append(a)
+        procs.append(p)
+    for c in conns:
+        assert c.recv() == "ready"
 
     def step():
-        # one Newton iteration of every sampled case (max_it = 1), one case per thread
         t = time.perf_counter()
-        oracle.runpf(buses, branches, sample, alg=0, max_it=1, solver=oracle.SOLVER_EIGEN, threads=threads)
-        return time.perf_counter() - t
+        for c in conns:
+            c.send("step")
+        rs = [c.recv() for c in conns]
+        return time.perf_counter() - t, rs
 
+    finished, fin_iters, fin_conv = 0, 0, 0
     for _ in range(args.warmup):
-        step()
-    times = [step() for _ in range(args.steps)]
-    per_step = sum(times) / len(times)
-    value = len(sample) / (iters * per_step)
+        _, rs = step()
+        for r in rs:
+            finished, fin_iters, fin_conv = finished + r[2], fin_iters + r[3], fin_conv + r[4]
+    wall, iters = 0.0, 0
+    for _ in range(args.steps):
+        dt, rs = step()
+        wall += dt
+        for r in rs:
+            iters += r[1]
+            finished, fin_iters, fin_conv = finished + r[2], fin_iters + r[3], fin_conv + r[4]
+    extra = 0
+    while finished == 0 and extra < 12:  # short runs: step on, untimed, until a case finishes
+        _, rs = step()
+        extra += 1
+        for r in rs:
+            finished, fin_iters, fin_conv = finished + r[2], fin_iters + r[3], fin_conv + r[4]
+    for c in conns:
+        c.send("stop")
+    for p in procs:
+        p.join(timeout=60)
+    if finished == 0:
+        return {"impl": "reference", "unavailable": "no reference solve finished within the run"}
+    per_solve = fin_iters / finished
+    value = iters / per_solve / wall
     return {
-        "impl": "reference", "metric": METRIC, "value": value,
-        "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": args.workload, "n_cases_sample": len(sample), "alg": "NR",
-                   "linear_solver": "Eigen 3.2.8 SparseLU<COLAMD> (reference's Eigen_SparseLU option)"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference",
-                         "sample": f"each step = one Newton iteration of {len(sample)} cases (one per thread); "
-                                   f"solves/s = cases / ({iters:.1f} iterations x step time)"},
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, committed fixture)",
+        "config": {"workload": f"{args.workload}: {n_cases} N-1 contingencies, NR to 1e-8 p.u.", "alg": "NR",
+                   "linear_solver": "Eigen 3.2.8 SparseLU<COLAMD>, compute() every iteration (the reference's "
+                                    "Eigen_SparseLU option; its default MKL DSS is unavailable on this box)"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} timed steps, each one Newton iteration of the reference's own "
+                                   f"mkl_* code on each of {cores} cores (one process per core); {finished} solves "
+                                   f"finished during the run ({fin_conv} converged), {per_solve:.2f} iterations per "
+                                   f"solve; solves/s = iterations / iterations per solve / time"
+                                   + ("" if fin_conv else "; the reference converges none of these cases: it takes "
+                                      "voltage angles as atan(y/x) (cuCangle, util/complexUtils.h:21-23) and its "
+                                      "Newton iterates pass 90 degrees, so each case stops at MAX_IT_NR = 10; value "
+                                      "counts finished cases")},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
