@@ -197,6 +197,22 @@ def accuracy(res, ref):
 
 METRIC = "N-1 PF solves/sec @1e-8 pu, 9241-bus synth: mixed vs plain FP64; HBM GB/s"
 
+# Real grids beside the synthetic headline: the reference's bundled MATPOWER cases
+# (tests/golden/matpower_cases.npz, converted by tests/golden/make_matpower_fixtures.py),
+# N-1 outages of non-bridge branches.
+REAL_WORKLOADS = {"pegase9241": ("case9241pegase", 1000), "pegase2869": ("case2869pegase", 1000),
+                  "pegase1354": ("case1354pegase", 1000)}
+
+
+def real_workload(name, rank=0, outage_seed=7):
+    import mapol_b200 as m
+
+    case, n_out = REAL_WORKLOADS[name]
+    g = np.load(os.path.join(ROOT, "tests", "golden", "matpower_cases.npz"))
+    buses, branches = g[case + "_buses"], g[case + "_branches"]
+    n_out = min(n_out, int((~m.find_bridges(branches, len(buses))).sum()))
+    return buses, branches, m.n1_cases(branches, len(buses), n_out, outage_seed + rank)
+
 
 def _ref_worker(conn, fixture, case_ids, solver):
     """One host core running the reference's own Newton-Raphson (oracle/_ref/librefpf.so,
@@ -324,7 +340,10 @@ def run_ours(args, rank, world, local_rank):
     from mapol_b200.shard import rank_cases
 
     torch.cuda.set_device(local_rank)
-    buses, branches, cases = rank_cases(args.workload, rank)
+    if args.workload in REAL_WORKLOADS:
+        buses, branches, cases = real_workload(args.workload, rank)
+    else:
+        buses, branches, cases = rank_cases(args.workload, rank)
     if args.cases:
         cases = cases[: args.cases]
     n_cases = len(cases)
@@ -449,7 +468,9 @@ def run_ours(args, rank, world, local_rank):
                                             "GB/s": round(b * units / (v / 1e3) / 1e9, 1) if v > 0 else None}
 
     line = {
-        "metric": METRIC,
+        "metric": METRIC if args.workload == WORKLOAD else METRIC.replace(
+            "9241-bus synth", REAL_WORKLOADS[args.workload][0] + " (real grid)" if args.workload in REAL_WORKLOADS
+            else args.workload),
         "value": value,
         "unit": "solves/s",
         "n_gpus": world,
@@ -460,7 +481,10 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64 mismatch/update/convergence test, f32 LU factorisation and solves",
-        "data": "synthetic (seeded generator: 9241 buses, 16049 branches, 1445 PV, 15% tapped)",
+        "data": ("synthetic (seeded generator: 9241 buses, 16049 branches, 1445 PV, 15% tapped)"
+                 if args.workload == WORKLOAD else
+                 f"real grid: the reference's bundled {REAL_WORKLOADS[args.workload][0]}.m"
+                 if args.workload in REAL_WORKLOADS else f"synthetic ({args.workload})"),
         "config": {"workload": f"{args.workload}: {n_cases} N-1 contingencies per GPU, NR to 1e-8 p.u.",
                    "n_cases_per_gpu": n_cases, "alg": "NR", "parallelism": f"replicas x{world} (cases sharded)",
                    "l2": "inputs larger than L2 (factor working set %.1f GB per GPU)" % (st["device_bytes"] / 1e9)},

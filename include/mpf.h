@@ -77,7 +77,10 @@ typedef enum mpf_case_status {
   MPF_CASE_CONVERGED = 1,  /* max |mismatch| < tol */
   MPF_CASE_MAX_ITER = 2,   /* iteration limit reached (the reference's "not converged") */
   MPF_CASE_DIVERGED = 3,   /* non-finite mismatch or voltage */
-  MPF_CASE_SINGULAR = 4    /* zero / tiny pivot in the LU */
+  MPF_CASE_SINGULAR = 4    /* zero / tiny pivot in the LU, or outages that cut PV / PQ
+                              buses off from every slack (found by mpf_set_cases: the
+                              Jacobian is structurally singular; such a case is not
+                              iterated and reports 0 iterations and its start point) */
 } mpf_case_status;
 
 /* Bus record: the fields of Bus (src/powersystem/Bus.h:18-31) the power flow reads. */
@@ -303,7 +306,9 @@ int32_t mpf_branch_flows(mpf_handle* h, double* ploss, double* overload, double*
  *   L = sum_k relu(|Sf_k| - 0.9 rating_k)^2        (needs mpf_set_ratings)
  * at the solved voltages of the last mpf_solve.  J is refactorised at the solution in
  * `precision` (MPF_FP64 or MPF_MIXED = FP32 factors) and J^T lambda = dL/dx is solved
- * with transposed substitutions on those factors.  Outputs (device, each nullable):
+ * with transposed substitutions on those factors; with FP32 factors the solution is
+ * refined twice with FP64 residuals dL/dx - J^T lambda (J refilled in FP64, whose
+ * buffer is allocated on first use), which brings it to FP64 accuracy.  Outputs (device, each nullable):
  *   grad_p, grad_q [n_cases][n_bus]     dL/dP, dL/dQ of the net injections (0 where the
  *                                       injection is not a Newton equation: slack, Q of PV)
  *   grad_g, grad_b [n_cases][n_branch]  dL/dg, dL/db of the series admittance g + jb =

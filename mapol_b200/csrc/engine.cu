@@ -14,11 +14,13 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <array>
 #include <climits>
 #include <mutex>
 #include <set>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -1122,11 +1124,18 @@ struct mpf_handle {
   DevBuf vout, small_out;
   DevBuf eval_acc;  // mpf_mismatch accumulator, allocated on first use
   DevBuf br_dy;     // per branch dY/dg for (ff, ft, tf, tt), adjoint
+  // adjoint refinement (FP32 factors): J^T by column (A-array position, row), the FP64
+  // right-hand side and solution, allocated on the first mixed-precision adjoint
+  DevBuf adj_colptr, adj_colent, adj_b64, adj_lam64;
   DevBuf adj_status;  // statuses the adjoint's refactorisation may write (kept apart)
   // several islands (grids) in one handle: per-bus / per-branch islands, and per
   // batch the island of each group and the case <-> lane maps
   DevBuf bus_island, br_island, group_island, lane_case, case_lane;
   std::vector<int> h_lane_case;
+  // cases whose outages island PV/PQ buses (no path to a slack): per lane, uploaded
+  // only when the batch has one; the grid's bridges make the single-outage check O(1)
+  DevBuf case_cut;
+  std::vector<uint8_t> is_bridge;
   // reactive limits: PV buses with limits (a Vm variable each), their limits, and per
   // batch the PV / switched state of each case
   int nsw = 0;
@@ -1218,6 +1227,7 @@ struct mpf_handle {
       d.q_fix = q_fix.as<double>();
       d.iter_base = iter_base.as<int>();
     }
+    if (case_cut.p) d.case_cut = case_cut.as<unsigned char>();
     if (ctl.nc > 0) {
       d.nslot = ctl.nslot;
       d.noltc = ctl.noltc;
@@ -1259,7 +1269,8 @@ struct mpf_handle {
                            &out_br, &sbus_case, &V, &Ibus, &status, &iters, &maxmis, &facc, &group_active,
                            &any_active, &vout, &small_out, &fdvar, &eval_acc, &it_ctr, &br_dy,
                            &adj_status, &bus_island, &br_island, &group_island, &lane_case, &case_lane,
-                           &sw_index, &sw_bus, &q_lim, &base_type, &pv_on, &q_fix, &q_flag, &iter_base};
+                           &sw_index, &sw_bus, &q_lim, &base_type, &pv_on, &q_fix, &q_flag, &iter_base, &case_cut,
+                           &adj_colptr, &adj_colent, &adj_b64, &adj_lam64};
     for (auto p : all) b += p->bytes;
     b += ctl.bytes();
     const LUSystem* systems[] = {&jac, &bp[0], &bp[1], &bpp[0], &bpp[1]};
@@ -1288,6 +1299,29 @@ void upload_newton(mpf_handle* h) {
   for (size_t p = 0; p < jp.size(); ++p)
     jp[p] = make_int4(g.jpos[4 * p], g.jpos[4 * p + 1], g.jpos[4 * p + 2], g.jpos[4 * p + 3]);
   upload(h->jpos, jp);
+  {
+    // J^T by column for the adjoint refinement: entry (row, col) of each A-array slot
+    // (jac_entry's quadrants: (P_i, Va_j), (P_i, Vm_j), (Q_i, Va_j), (Q_i, Vm_j))
+    std::vector<std::array<int, 3>> ent;  // (col, row, A-array position)
+    for (int i = 0; i < g.nb; ++i)
+      for (int p = g.y_rowptr[i]; p < g.y_rowptr[i + 1]; ++p) {
+        const int j = g.y_col[p];
+        const int rows[4] = {g.var_va[i], g.var_va[i], g.var_vm[i], g.var_vm[i]};
+        const int cols[4] = {g.var_va[j], g.var_vm[j], g.var_va[j], g.var_vm[j]};
+        for (int q = 0; q < 4; ++q)
+          if (g.jpos[4 * p + q] >= 0) ent.push_back({cols[q], rows[q], g.jpos[4 * p + q]});
+      }
+    std::sort(ent.begin(), ent.end());
+    std::vector<int> cp(g.jac.n + 1, 0);
+    std::vector<int2> ce(ent.size());
+    for (size_t e = 0; e < ent.size(); ++e) {
+      ++cp[ent[e][0] + 1];
+      ce[e] = make_int2(ent[e][2], ent[e][1]);
+    }
+    for (int c = 0; c < g.jac.n; ++c) cp[c + 1] += cp[c];
+    upload(h->adj_colptr, cp);
+    upload(h->adj_colent, ce);
+  }
   if (g.n_islands > 1) {
     std::vector<int> vi(g.jac.n, -1);
     for (int i = 0; i < g.nb; ++i) {
@@ -1698,6 +1732,10 @@ void launch_bsolve_t(const LUSystem& sys, int ngroups, const T* pan, T* x, const
   }
 }
 
+// Refinement steps of the adjoint solved with FP32 factors (each reduces the error by
+// about the FP32 LU's own accuracy, ~1e-4 relative on the 1354-bus grid).
+constexpr int kAdjRefine = 2;
+
 // J of the solved point refactorised in T, then J^T lambda = dL/dx by U^T (bottom-up)
 // and L^T (top-down) substitutions, then the bus and branch gradients.
 template <typename T>
@@ -1710,6 +1748,7 @@ void adjoint_impl(mpf_handle* h, cudaStream_t st, double* gp, double* gq, double
   T* x = J.x[P].as<T>();
   const int lanes = h->ngroups * 32;
   if (!h->adj_status.p || h->adj_status.bytes < lanes * sizeof(int)) h->adj_status.alloc(lanes * sizeof(int));
+  CUDA_TRY(cudaMemsetAsync(h->adj_status.p, 0, lanes * sizeof(int), st));  // all RUNNING: a sink for bad pivots
   DevGrid d = h->dev();
   k_fill_int<<<(h->ngroups + 255) / 256, 256, 0, st>>>(d.group_active, h->ngroups, 1);
   CUDA_TRY(cudaGetLastError());
@@ -1718,21 +1757,61 @@ void adjoint_impl(mpf_handle* h, cudaStream_t st, double* gp, double* gq, double
   int nl = 0;
   launch_factor<T>(J, h->ngroups, A, pan, J.cb[P].as<T>(), J.cbr[P].as<T>(), x, h->adj_status.as<int>(),
                    d.group_active, 0, st, &nl);
-  CUDA_TRY(cudaMemsetAsync(x, 0, (size_t)lanes * J.sym.n * sizeof(T), st));
+  const size_t nx = (size_t)lanes * J.sym.n;
   const dim3 bg((unsigned)((h->g.nbr + 63) / 64), (unsigned)h->ngroups);
-  k_adj_dldx<T><<<bg, 256, 0, st>>>(d, h->g.nbr, h->rating.as<double>(), x);
-  CUDA_TRY(cudaGetLastError());
-  launch_fsolve_t<T>(J, h->ngroups, pan, J.cbr[P].as<T>(), x, d.group_active, st);
-  launch_bsolve_t<T>(J, h->ngroups, pan, x, d.group_active, st);
-  if (gp || gq) {
-    const size_t total = (size_t)h->ncases * h->g.nb;
-    k_adj_grad_bus<T><<<(unsigned)std::min<size_t>(148 * 16, total / 256 + 1), 256, 0, st>>>(d, h->ncases, x, gp, gq);
+  auto gradients = [&](const auto* lam) {
+    using L = std::remove_cv_t<std::remove_pointer_t<decltype(lam)>>;
+    if (gp || gq) {
+      const size_t total = (size_t)h->ncases * h->g.nb;
+      k_adj_grad_bus<L><<<(unsigned)std::min<size_t>(148 * 16, total / 256 + 1), 256, 0, st>>>(d, h->ncases, lam, gp,
+                                                                                                 gq);
+      CUDA_TRY(cudaGetLastError());
+    }
+    if (gg || gb) {
+      k_adj_grad_branch<L><<<bg, 256, 0, st>>>(d, h->g.nbr, h->ncases, h->rating.as<double>(),
+                                               h->br_dy.as<double2>(), lam, gg, gb);
+      CUDA_TRY(cudaGetLastError());
+    }
+  };
+  if constexpr (std::is_same<T, double>::value) {
+    CUDA_TRY(cudaMemsetAsync(x, 0, nx * sizeof(T), st));
+    k_adj_dldx<T><<<bg, 256, 0, st>>>(d, h->g.nbr, h->rating.as<double>(), x);
     CUDA_TRY(cudaGetLastError());
-  }
-  if (gg || gb) {
-    k_adj_grad_branch<T><<<bg, 256, 0, st>>>(d, h->g.nbr, h->ncases, h->rating.as<double>(),
-                                             h->br_dy.as<double2>(), x, gg, gb);
+    launch_fsolve_t<T>(J, h->ngroups, pan, J.cbr[P].as<T>(), x, d.group_active, st);
+    launch_bsolve_t<T>(J, h->ngroups, pan, x, d.group_active, st);
+    gradients(x);
+  } else {
+    // FP32 factors: solve, then refine with FP64 residuals of the FP64 Jacobian
+    J.ensure_values(0, h->ngroups);
+    double* A64 = J.A[0].as<double>();
+    if (!h->adj_b64.p || h->adj_b64.bytes < nx * sizeof(double)) {
+      h->adj_b64.alloc(nx * sizeof(double));
+      h->adj_lam64.alloc(nx * sizeof(double));
+    }
+    double* b64 = h->adj_b64.as<double>();
+    double* lam64 = h->adj_lam64.as<double>();
+    // entries of other islands are never filled: start from zeros so they stay finite
+    CUDA_TRY(cudaMemsetAsync(A64, 0, (size_t)lanes * J.nA * sizeof(double), st));
+    launch_mismatch_nr<double>(d, rg, st, J.x[0].as<double>(), A64, true);
+    CUDA_TRY(cudaMemsetAsync(b64, 0, nx * sizeof(double), st));
+    k_adj_dldx<double><<<bg, 256, 0, st>>>(d, h->g.nbr, h->rating.as<double>(), b64);
     CUDA_TRY(cudaGetLastError());
+    const unsigned eb = (unsigned)std::min<size_t>(148 * 16, nx / 256 + 1);
+    k_adj_cast<T><<<eb, 256, 0, st>>>(nx, b64, x);
+    CUDA_TRY(cudaGetLastError());
+    const dim3 cgrid((unsigned)((J.sym.n + 7) / 8), (unsigned)h->ngroups);
+    for (int r = 0; r <= kAdjRefine; ++r) {
+      if (r > 0) {
+        k_adj_residual<T><<<cgrid, 256, 0, st>>>(J.sym.n, h->ngroups, J.nA, h->adj_colptr.as<int>(),
+                                                 h->adj_colent.as<int2>(), A64, lam64, b64, x);
+        CUDA_TRY(cudaGetLastError());
+      }
+      launch_fsolve_t<T>(J, h->ngroups, pan, J.cbr[P].as<T>(), x, d.group_active, st);
+      launch_bsolve_t<T>(J, h->ngroups, pan, x, d.group_active, st);
+      k_adj_accumulate<T><<<eb, 256, 0, st>>>(nx, x, lam64, r > 0);
+      CUDA_TRY(cudaGetLastError());
+    }
+    gradients(lam64);
   }
 }
 
@@ -1794,6 +1873,8 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
     if (!msg.empty()) return fail(h.get(), MPF_ERR_BAD_INPUT, msg);
     h->buses.assign(buses, buses + n_bus);
     h->branches.assign(branches, branches + n_branch);
+    if (find_bridges(branches, n_branch, n_bus, h->is_bridge) != 0)
+      return fail(h.get(), MPF_ERR_BAD_INPUT, "bridge search failed");
     const GridSymbolic& g = h->g;
     int maxf = g.jac.max_front;
     for (int v = 0; v < 2; ++v) maxf = std::max({maxf, g.bp[v].lu.max_front, g.bpp[v].lu.max_front});
@@ -1995,6 +2076,55 @@ int set_cases_impl(mpf_handle* h, int32_t n_cases, const int32_t* island_of_case
         maxk = std::max(maxk, e - b);
       }
     }
+    // cases whose outages cut PV/PQ buses off from every slack: a non-bridge single
+    // outage never does; otherwise search from the slacks over the remaining branches
+    std::vector<unsigned char> cut(lanes, 0);
+    bool any_cut = false;
+    if (outage_offsets) {
+      std::vector<std::vector<int>> adj;  // built on first need
+      std::vector<int> seen(g.nb, -1), stack;
+      for (int c = 0; c < n_cases; ++c) {
+        const int b = outage_offsets[c], e = outage_offsets[c + 1];
+        if (e == b || (e - b == 1 && !h->is_bridge[outage_branches[b]])) continue;
+        if (adj.empty()) {
+          adj.resize(g.nb);
+          for (int k = 0; k < g.nbr; ++k)
+            if (h->branches[k].status != 0) {
+              adj[h->branches[k].from].push_back(k);
+              adj[h->branches[k].to].push_back(k);
+            }
+        }
+        auto out_here = [&](int k) {
+          for (int q = b; q < e; ++q)
+            if (outage_branches[q] == k) return true;
+          return false;
+        };
+        stack.clear();
+        for (int i = 0; i < g.nb; ++i)
+          if (g.bus_type[i] == MPF_BUS_SLACK) {
+            seen[i] = c;
+            stack.push_back(i);
+          }
+        while (!stack.empty()) {
+          const int i = stack.back();
+          stack.pop_back();
+          for (int k : adj[i]) {
+            if (out_here(k)) continue;
+            const int j = h->branches[k].from == i ? h->branches[k].to : h->branches[k].from;
+            if (seen[j] != c) {
+              seen[j] = c;
+              stack.push_back(j);
+            }
+          }
+        }
+        for (int i = 0; i < g.nb; ++i)
+          if (seen[i] != c && (g.bus_type[i] == MPF_BUS_PV || g.bus_type[i] == MPF_BUS_PQ)) {
+            cut[case_lane[c]] = 1;
+            any_cut = true;
+            break;
+          }
+      }
+    }
     std::vector<double2> sb;
     if (sbus) {
       sb.assign((size_t)ngroups * g.nb * 32, make_double2(0.0, 0.0));
@@ -2025,6 +2155,8 @@ int set_cases_impl(mpf_handle* h, int32_t n_cases, const int32_t* island_of_case
       }
     }
     upload(h->out_br, outs);
+    if (any_cut) upload(h->case_cut, cut);
+    else h->case_cut.release();
     if (sbus) upload(h->sbus_case, sb);
     else h->sbus_case.release();
     if (multi) {

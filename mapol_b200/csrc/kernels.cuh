@@ -85,6 +85,9 @@ struct DevGrid {
   unsigned char* pv_on;     // [g][nsw][32] 1 while PV in that case, 0 once switched to PQ
   double* q_fix;            // [g][nsw][32] Q the switched bus holds (its violated limit)
   int* iter_base;           // [ngroups*32] Newton iterations of the case's earlier rounds
+  // cases whose outages cut PV/PQ buses off from every slack (their Jacobian is
+  // structurally singular): SINGULAR from the start, never iterated (null: none)
+  const unsigned char* case_cut;  // [ngroups*32]
 };
 
 __device__ __forceinline__ bool row_here(const DevGrid& d, int i, int g) {
@@ -138,6 +141,11 @@ __device__ __forceinline__ bool task_here(const DevLU& L, int s, int g) {
 }
 
 // ---------------------------------------------------------------- helpers
+// A zero or non-finite pivot ends a running case as SINGULAR.  The factorisation runs
+// on whole groups of 32 lanes, so lanes whose case already finished (converged,
+// diverged, or cut off at set-up) are factored too; their status stays as it is.
+__device__ __forceinline__ void mark_singular(int* st) { atomicCAS(st, (int)ST_RUNNING, (int)ST_SINGULAR); }
+
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -258,7 +266,7 @@ __global__ void k_init(DevGrid d, int ncases) {
   }
   const int nl = d.ngroups * 32;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nl; c += gridDim.x * blockDim.x) {
-    d.status[c] = case_of_lane(d, c, ncases) >= 0 ? ST_RUNNING : ST_CONVERGED;
+    d.status[c] = case_of_lane(d, c, ncases) < 0 ? ST_CONVERGED : (d.case_cut && d.case_cut[c] ? ST_SINGULAR : ST_RUNNING);
     d.iters[c] = 0;
     d.maxmis[c] = 0.0;
     d.facc[c] = 0ull;
@@ -607,7 +615,7 @@ __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int
     for (int k = 0; k < V; ++k) {
       T pk = piv.v[k];
       if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
-        if (lead) st_lanes[k] = ST_SINGULAR;
+        if (lead) mark_singular(&st_lanes[k]);
         pk = (T)1;
       }
       inv.v[k] = (T)1 / pk;
@@ -809,7 +817,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
       for (int k = 0; k < V; ++k) {
         T pk = piv.v[k];
         if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
-          if (slot == 0) status[g * 32 + lane + k] = ST_SINGULAR;
+          if (slot == 0) mark_singular(&status[g * 32 + lane + k]);
           pk = (T)1;
         }
         inv.v[k] = (T)1 / pk;
@@ -959,7 +967,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
       for (int k = 0; k < V; ++k) {
         T pk = piv.v[k];
         if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
-          if (slot == 0) status[g * 32 + lane + k] = ST_SINGULAR;
+          if (slot == 0) mark_singular(&status[g * 32 + lane + k]);
           pk = (T)1;
         }
         inv.v[k] = (T)1 / pk;
@@ -1414,6 +1422,43 @@ __global__ void __launch_bounds__(256) k_adj_dldx(DevGrid d, int nbr, const doub
     if (vfv.y >= 0 && !still_pv(d, ft.x, grp, lane)) atomicAdd(&g[at32(grp, d.n_jac, vfv.y, lane)], (T)dvm_f);
     if (vtv.y >= 0 && !still_pv(d, ft.y, grp, lane)) atomicAdd(&g[at32(grp, d.n_jac, vtv.y, lane)], (T)(cc * swr / mt));
   }
+}
+
+// Iterative refinement of the adjoint solved with FP32 factors: the residual
+// r = b - J^T lam is formed in FP64 with the Jacobian refilled in FP64 at the same
+// point, solved again with the FP32 factors and added to lam (FP64), so the FP32 LU
+// only has to reduce the error by its own accuracy at each step.  Column c of J^T lam
+// gathers the J entries of variable c: col_ptr / col_ent list, per column, the
+// A-array position and the row (equation) of each entry.  Warp = column x 32 lanes.
+template <typename T>
+__global__ void __launch_bounds__(256) k_adj_residual(int n, int ngroups, int nA, const int* __restrict__ col_ptr,
+                                                      const int2* __restrict__ col_ent, const double* __restrict__ A,
+                                                      const double* __restrict__ lam, const double* __restrict__ b,
+                                                      T* __restrict__ r) {
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int g = blockIdx.y;
+  if (col >= n || g >= ngroups) return;
+  double s = b[at32(g, n, col, lane)];
+  for (int q = col_ptr[col]; q < col_ptr[col + 1]; ++q) {
+    const int2 e = col_ent[q];  // (A-array position, row)
+    s -= A[at32(g, nA, e.x, lane)] * lam[at32(g, n, e.y, lane)];
+  }
+  r[at32(g, n, col, lane)] = (T)s;
+}
+
+// lam (FP64) = or += the FP32 correction x; n_total entries
+template <typename T>
+__global__ void k_adj_accumulate(size_t n_total, const T* __restrict__ x, double* __restrict__ lam, int add) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n_total; t += (size_t)gridDim.x * blockDim.x)
+    lam[t] = (add ? lam[t] : 0.0) + (double)x[t];
+}
+
+// x (T) = b (FP64)
+template <typename T>
+__global__ void k_adj_cast(size_t n_total, const double* __restrict__ b, T* __restrict__ x) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n_total; t += (size_t)gridDim.x * blockDim.x)
+    x[t] = (T)b[t];
 }
 
 // U^T z = g, supernodes bottom-up (thread per case, warp per (supernode, group)):

@@ -1,4 +1,5 @@
-"""Converts the reference's bundled MATPOWER cases (src/datasets/case14, 30, 118, 300)
+"""Converts the reference's bundled MATPOWER cases (src/datasets/case14, 30, 57, 118, 300,
+case1354pegase, case2869pegase, case9241pegase)
 with mapol_b200.matpower.load_matpower (and the generators' Q limits, q_limits) into
 tests/golden/matpower_cases.npz, so the GPU tests can run real grids where the reference
 tree is absent.  Run from the repository root:
@@ -19,7 +20,7 @@ SRC = "/root/reference/src/datasets"
 
 def main():
     out = {}
-    for name in ("case14", "case30", "case118", "case300"):
+    for name in ("case14", "case30", "case57", "case118", "case300", "case1354pegase", "case2869pegase", "case9241pegase"):
         buses, branches, rating = load_matpower(os.path.join(SRC, name + ".m"))
         out[name + "_buses"] = buses
         out[name + "_branches"] = branches

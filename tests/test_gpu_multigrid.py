@@ -44,6 +44,24 @@ def test_three_grids_one_batch_match_oracle(cfg2, alg):
                 _compare(res, ref, 0 if prec == m.FP64 else 1, tight)
 
 
+def test_config2_full_size_matches_oracle(gpu):
+    """Config 2 at its stated size: the 118-, 1354- and 2869-bus grids with 167 / 400 /
+    400 N-1 cases in one batch (167 = every non-bridge branch of the 118-bus grid, of
+    the 200 asked for), Newton-Raphson in both precisions, each grid against the oracle."""
+    grids, cases = m.grid.workload_set("cfg2")
+    assert [len(c) for c in cases] == [167, 400, 400]
+    refs = [oracle.runpf(b, br, cs, alg=m.NR) for (b, br), cs in zip(grids, cases)]
+    with m.MultiGrid(grids) as mg:
+        mg.set_cases(cases)
+        for prec in (m.FP64, m.MIXED):
+            mg.solve(m.NR, prec)
+            for res, ref, (b, br), cs in zip(mg.results(), refs, grids, cases):
+                tight = lambda idx, b=b, br=br, cs=cs: oracle.runpf(b, br, [cs[i] for i in idx], alg=m.NR,
+                                                                    tol=TIGHT_TOL)
+                conv = _compare(res, ref, 0 if prec == m.FP64 else 1, tight)
+                assert conv.all()
+
+
 def test_one_batch_launches_like_its_largest_grid(cfg2):
     """The stages of all grids share launches: a three-grid solve launches about as
     many kernels as its largest grid alone, not the sum of the three."""
