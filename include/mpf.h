@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define MPF_ABI_VERSION 2
+#define MPF_ABI_VERSION 3
 
 /* algorithms — same values as NR / FDXB / FDBX in src/powerflow/runpf.h:16-18 */
 #define MPF_NR   0
@@ -117,8 +117,19 @@ typedef struct mpf_options {
   int32_t autotune;    /* 1: time the candidate kernels of every factorisation launch on
                           the first solve of a batch size and keep the fastest (default 1);
                           0: fixed heuristic */
-  int32_t reserved[4];
+  int32_t ordering;    /* fill-reducing bus order of the Newton system, MPF_ORDER_*:
+                          0 automatic (default), 1 minimum degree, 2 minimum fill,
+                          3 minimum fill weighted by variables per bus */
+  int32_t reserved[3];
 } mpf_options;
+
+/* orderings (mpf_options.ordering).  Automatic: the candidate with the least estimated
+ * factorisation time per case, flops + 53000 x elimination-tree levels (a level costs
+ * about one launch of the level-synchronous factorisation and backward solve). */
+#define MPF_ORDER_AUTO 0
+#define MPF_ORDER_MIN_DEGREE 1
+#define MPF_ORDER_MIN_FILL 2
+#define MPF_ORDER_MIN_FILL_WEIGHTED 3
 
 /* Per-kernel device time of the last mpf_solve (CUDA events on the solve stream),
  * milliseconds, summed over all launches of that kernel in the solve. */
@@ -142,6 +153,8 @@ typedef struct mpf_stats {
   int64_t nnz_lu_upper;                        /* entries of the Newton system's U panels (the
                                                   pivot rows of each supernode: what a backward
                                                   substitution reads) */
+  int32_t ordering;                            /* MPF_ORDER_* the Newton system uses */
+  int32_t pad_;
 } mpf_stats;
 
 typedef struct mpf_handle mpf_handle;

@@ -45,6 +45,8 @@ FP64, MIXED = 0, 1
 MAX_IT_NR, MAX_IT_FD, EPS = 10, 30, 1e-8
 
 CASE_RUNNING, CASE_CONVERGED, CASE_MAX_ITER, CASE_DIVERGED, CASE_SINGULAR = 0, 1, 2, 3, 4
+# fill-reducing orderings of the Newton system (mpf_options.ordering)
+ORDER_AUTO, ORDER_MIN_DEGREE, ORDER_MIN_FILL, ORDER_MIN_FILL_WEIGHTED = 0, 1, 2, 3
 # per-case control kinds (the values of Particula::Estrutura::Tipo, src/pso/Particula.h:27-29)
 CTRL_AVR, CTRL_OLTC, CTRL_SHC = 1, 2, 3
 CONTROL_DTYPE = np.dtype([("kind", "<i4"), ("index", "<i4")])
@@ -84,7 +86,8 @@ class Options(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
         ("autotune", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("ordering", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -125,4 +128,6 @@ class Stats(ctypes.Structure):
         ("case_groups", ctypes.c_int32),
         ("device_bytes", ctypes.c_int64),
         ("nnz_lu_upper", ctypes.c_int64),
+        ("ordering", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
     ]

@@ -1858,7 +1858,8 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
   mpf_default_options(&h->opt);
   if (opt) h->opt = *opt;
   if (h->opt.max_it_nr < 0 || h->opt.max_it_fd < 0 || !(h->opt.tol > 0.0) ||
-      (h->opt.angle_mode != 0 && h->opt.angle_mode != 1)) {
+      (h->opt.angle_mode != 0 && h->opt.angle_mode != 1) || h->opt.ordering < MPF_ORDER_AUTO ||
+      h->opt.ordering > MPF_ORDER_MIN_FILL_WEIGHTED) {
     h->err = "invalid options";
     *out = h.release();
     return MPF_ERR_BAD_INPUT;
@@ -1869,7 +1870,7 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
     if (h->opt.device < 0 || h->opt.device >= ndev) return fail(h.get(), MPF_ERR_BAD_INPUT, "device ordinal out of range");
     h->device = h->opt.device;
     CUDA_TRY(cudaSetDevice(h->device));
-    const std::string msg = build_symbolic(buses, n_bus, branches, n_branch, h->g);
+    const std::string msg = build_symbolic(buses, n_bus, branches, n_branch, h->g, nullptr, h->opt.ordering);
     if (!msg.empty()) return fail(h.get(), MPF_ERR_BAD_INPUT, msg);
     h->buses.assign(buses, buses + n_bus);
     h->branches.assign(branches, branches + n_branch);
@@ -1980,6 +1981,7 @@ int32_t mpf_get_stats(const mpf_handle* h, mpf_stats* st) {
   st->case_groups = h->ngroups;
   st->device_bytes = (int64_t)h->device_bytes();
   for (int s = 0; s < g.jac.nsn; ++s) st->nnz_lu_upper += (int64_t)g.jac.sn_w[s] * g.jac.sn_f[s];
+  st->ordering = g.ordering;
   return MPF_OK;
 }
 
@@ -2365,7 +2367,7 @@ int32_t mpf_set_q_limits(mpf_handle* h, const double* qmin, const double* qmax) 
     // the Newton system with a Vm variable and a Q equation for every limited PV bus
     GridSymbolic g2;
     const std::string msg = build_symbolic(h->buses.data(), nb, h->branches.data(), (int)h->branches.size(), g2,
-                                           swb.empty() ? nullptr : &vf);
+                                           swb.empty() ? nullptr : &vf, h->opt.ordering);
     if (!msg.empty()) return fail(h, MPF_ERR_BAD_INPUT, msg);
     if (g2.jac.max_front > kFmaxAll)
       return fail(h, MPF_ERR_BAD_INPUT, "largest frontal matrix with the limited PV buses exceeds " +

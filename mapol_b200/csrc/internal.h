@@ -109,6 +109,12 @@ void arrowhead_layout(const LUSymbolic& s, const std::vector<int>& rows,
 // loops).  Returns perm with perm[k] = vertex eliminated k-th.  Ties: lowest index.
 std::vector<int> minimum_degree(int n, const std::vector<std::vector<int>>& adj);
 
+// Minimum-deficiency (minimum fill-in) ordering: eliminates next the vertex whose
+// elimination adds the fewest edges among its neighbours, each missing edge (a, b)
+// counted weight[a] x weight[b] (weight null: 1).  Ties: smaller weighted degree,
+// then lowest index.  Returns perm as minimum_degree.
+std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj, const std::vector<int>* weight);
+
 // Everything that does not depend on the case batch.
 struct GridSymbolic {
   int nb = 0, nbr = 0, npv = 0, npq = 0, slack = -1, n_slack = 0;
@@ -129,6 +135,7 @@ struct GridSymbolic {
 
   // Newton system: variables = Va of every PV/PQ bus, Vm of every PQ bus
   std::vector<int> bus_order;        // elimination order of PV/PQ buses
+  int ordering = 0;                  // the method that produced it (MPF_ORDER_*)
   std::vector<int> var_va, var_vm;   // per bus: LU variable index or -1
   LUSymbolic jac;
   int nnz_jac = 0;
@@ -156,8 +163,10 @@ struct GridSymbolic {
 // Validates the grid and fills g.  Returns empty string on success, else a message.
 // vm_free (nullable): PV buses that also get a Vm variable and a Q equation (buses
 // whose reactive limits may switch them to PQ).
+// ordering: MPF_ORDER_* of the Newton system's bus elimination order (AUTO picks the
+// candidate with the least estimated factorisation time).
 std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, int nbr,
-                           GridSymbolic& g, const std::vector<char>* vm_free = nullptr);
+                           GridSymbolic& g, const std::vector<char>* vm_free = nullptr, int ordering = 0);
 
 }  // namespace mpf
 

@@ -16,6 +16,7 @@
 #include <functional>
 #include <set>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "internal.h"
@@ -77,6 +78,89 @@ std::vector<int> minimum_degree(int n, const std::vector<std::vector<int>>& adj0
     }
     adj[v].clear();
     adj[v].shrink_to_fit();
+  }
+  return perm;
+}
+
+std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj0, const std::vector<int>* weight) {
+  std::vector<std::vector<int>> adj(n);
+  for (int v = 0; v < n; ++v)
+    for (int a : adj0[v])
+      if (a != v) {
+        adj[v].push_back(a);
+        adj[a].push_back(v);
+      }
+  for (auto& a : adj) {
+    std::sort(a.begin(), a.end());
+    a.erase(std::unique(a.begin(), a.end()), a.end());
+  }
+  auto W = [&](int v) -> long long { return weight ? (*weight)[v] : 1; };
+  std::vector<int> mark(n, -1);
+  int stamp = 0;
+  // weighted count of the edges that eliminating v would add (pairs of its
+  // neighbours not yet adjacent)
+  auto fill_of = [&](int v) {
+    long long f = 0;
+    const std::vector<int>& nb = adj[v];
+    for (size_t i = 0; i + 1 < nb.size(); ++i) {
+      ++stamp;
+      for (int x : adj[nb[i]]) mark[x] = stamp;
+      for (size_t j = i + 1; j < nb.size(); ++j)
+        if (mark[nb[j]] != stamp) f += W(nb[i]) * W(nb[j]);
+    }
+    return f;
+  };
+  auto degree_of = [&](int v) {
+    long long d = 0;
+    for (int a : adj[v]) d += W(a);
+    return d;
+  };
+  std::vector<long long> fill(n), deg(n);
+  std::set<std::tuple<long long, long long, int>> pq;
+  for (int v = 0; v < n; ++v) {
+    fill[v] = fill_of(v);
+    deg[v] = degree_of(v);
+    pq.insert({fill[v], deg[v], v});
+  }
+  std::vector<int> perm;
+  perm.reserve(n);
+  std::vector<char> done(n, 0);
+  std::vector<int> tmp, touched;
+  std::vector<int> seen(n, -1);
+  while (!pq.empty()) {
+    const int v = std::get<2>(*pq.begin());
+    pq.erase(pq.begin());
+    perm.push_back(v);
+    done[v] = 1;
+    const std::vector<int> nv = adj[v];
+    for (int a : nv) {
+      // adj[a] <- (adj[a] u nv) \ {a, v}: the neighbours of v become a clique
+      tmp.clear();
+      std::set_union(adj[a].begin(), adj[a].end(), nv.begin(), nv.end(), std::back_inserter(tmp));
+      adj[a].clear();
+      for (int u : tmp)
+        if (u != a && u != v) adj[a].push_back(u);
+    }
+    adj[v].clear();
+    // the fill of every vertex within two steps of v may have changed
+    touched.clear();
+    for (int a : nv) {
+      if (seen[a] != v) {
+        seen[a] = v;
+        touched.push_back(a);
+      }
+      for (int b : adj[a])
+        if (!done[b] && seen[b] != v) {
+          seen[b] = v;
+          touched.push_back(b);
+        }
+    }
+    for (int u : touched) {
+      pq.erase({fill[u], deg[u], u});
+      fill[u] = fill_of(u);
+      deg[u] = degree_of(u);
+      pq.insert({fill[u], deg[u], u});
+    }
   }
   return perm;
 }
@@ -377,7 +461,7 @@ static void build_fd(GridSymbolic& g, const mpf_bus* buses, const mpf_branch* br
 }
 
 std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, int nbr,
-                           GridSymbolic& g, const std::vector<char>* vm_free) {
+                           GridSymbolic& g, const std::vector<char>* vm_free, int ordering) {
   g = GridSymbolic();
   if (nb < 2) return "grid needs at least 2 buses";
   if (nbr < 1) return "grid needs at least 1 branch";
@@ -558,42 +642,76 @@ std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, i
       if (j != i && free_idx[j] >= 0) badj[a].push_back(free_idx[j]);
     }
   }
-  const std::vector<int> border = minimum_degree(nfree, badj);
-  g.bus_order.resize(nfree);
-  g.var_va.assign(nb, -1);
-  g.var_vm.assign(nb, -1);
-  int nv = 0;
-  for (int k = 0; k < nfree; ++k) {
-    const int i = free_bus[border[k]];
-    g.bus_order[k] = i;
-    g.var_va[i] = nv++;
-    // Vm is a variable of every PQ bus, and of PV buses that may switch to PQ (their
-    // Q limits are enforced): a superset pattern shared by all cases
-    if (g.bus_type[i] == MPF_BUS_PQ || (vm_free && (*vm_free)[i] && g.bus_type[i] == MPF_BUS_PV))
-      g.var_vm[i] = nv++;
-  }
-  // variable adjacency
-  std::vector<std::vector<int>> vadj(nv);
-  for (int i : g.bus_order) {
-    const int vi[2] = {g.var_va[i], g.var_vm[i]};
-    if (vi[1] >= 0) {
-      vadj[vi[0]].push_back(vi[1]);
-      vadj[vi[1]].push_back(vi[0]);
+  // Vm is a variable of every PQ bus, and of PV buses that may switch to PQ (their Q
+  // limits are enforced): a superset pattern shared by all cases
+  auto has_vm = [&](int i) {
+    return g.bus_type[i] == MPF_BUS_PQ || (vm_free && (*vm_free)[i] && g.bus_type[i] == MPF_BUS_PV);
+  };
+  // the Newton system's numbering and symbolic LU for one bus elimination order
+  auto newton_symbolic = [&](const std::vector<int>& border) {
+    g.bus_order.resize(nfree);
+    g.var_va.assign(nb, -1);
+    g.var_vm.assign(nb, -1);
+    int nv = 0;
+    for (int k = 0; k < nfree; ++k) {
+      const int i = free_bus[border[k]];
+      g.bus_order[k] = i;
+      g.var_va[i] = nv++;
+      if (has_vm(i)) g.var_vm[i] = nv++;
     }
-    for (int p = g.y_rowptr[i]; p < g.y_rowptr[i + 1]; ++p) {
-      const int j = g.y_col[p];
-      if (j == i || free_idx[j] < 0) continue;
-      const int vj[2] = {g.var_va[j], g.var_vm[j]};
-      for (int a : vi)
-        for (int b : vj)
-          if (a >= 0 && b >= 0) vadj[a].push_back(b);
+    std::vector<std::vector<int>> vadj(nv);
+    for (int i : g.bus_order) {
+      const int vi[2] = {g.var_va[i], g.var_vm[i]};
+      if (vi[1] >= 0) {
+        vadj[vi[0]].push_back(vi[1]);
+        vadj[vi[1]].push_back(vi[0]);
+      }
+      for (int p = g.y_rowptr[i]; p < g.y_rowptr[i + 1]; ++p) {
+        const int j = g.y_col[p];
+        if (j == i || free_idx[j] < 0) continue;
+        const int vj[2] = {g.var_va[j], g.var_vm[j]};
+        for (int a : vi)
+          for (int b : vj)
+            if (a >= 0 && b >= 0) vadj[a].push_back(b);
+      }
+    }
+    for (auto& a : vadj) {
+      std::sort(a.begin(), a.end());
+      a.erase(std::unique(a.begin(), a.end()), a.end());
+    }
+    lu_symbolic(nv, vadj, g.jac);
+  };
+  // Bus elimination order.  Candidates: minimum degree; minimum fill (deficiency); and
+  // minimum fill with each bus weighted by its variables (2 for a bus with Va and Vm, 1
+  // for Va alone), which counts the fill of the Newton system itself.  Automatic choice:
+  // the candidate with the least estimated factorisation time per case,
+  //   flops + kLevelFlops x levels,
+  // a level (one launch of the level-synchronous factorisation and backward solve)
+  // costing about as much as 53k flops per case: fitted on measured B200 times of the
+  // 9241-bus synthetic workload and case9241pegase, 1000 N-1 cases each, four orderings
+  // (factorisation + backward solve = 3.24 ms per MFLOP per case + 0.172 ms per level).
+  std::vector<int> wvar(nfree);
+  for (int a = 0; a < nfree; ++a) wvar[a] = has_vm(free_bus[a]) ? 2 : 1;
+  auto order_of = [&](int method) {
+    if (method == MPF_ORDER_MIN_FILL) return minimum_fill(nfree, badj, nullptr);
+    if (method == MPF_ORDER_MIN_FILL_WEIGHTED) return minimum_fill(nfree, badj, &wvar);
+    return minimum_degree(nfree, badj);
+  };
+  int method = ordering;
+  if (method == MPF_ORDER_AUTO) {
+    constexpr double kLevelFlops = 53000.0;
+    double best = 0.0;
+    for (int m : {MPF_ORDER_MIN_DEGREE, MPF_ORDER_MIN_FILL, MPF_ORDER_MIN_FILL_WEIGHTED}) {
+      newton_symbolic(order_of(m));
+      const double cost = (double)g.jac.flops + kLevelFlops * g.jac.nlevels;
+      if (method == MPF_ORDER_AUTO || cost < best) {
+        best = cost;
+        method = m;
+      }
     }
   }
-  for (auto& a : vadj) {
-    std::sort(a.begin(), a.end());
-    a.erase(std::unique(a.begin(), a.end()), a.end());
-  }
-  lu_symbolic(nv, vadj, g.jac);
+  newton_symbolic(order_of(method));
+  g.ordering = method;
   // J entries: the (Va,Va), (Va,Vm), (Vm,Va), (Vm,Vm) quadrants of every Ybus entry
   // between PV/PQ buses (newtonpf.h:215-295 enumerate the same set)
   std::vector<int> jr, jc, jsrc;

@@ -45,13 +45,14 @@ class PowerFlow:
     """One grid on one GPU (mpf_create).  Replaces hybrid_init / hybrid_free."""
 
     def __init__(self, buses, branches, max_it_nr=MAX_IT_NR, max_it_fd=MAX_IT_FD, tol=EPS,
-                 angle_mode=0, device=0, use_graph=1, autotune=1):
+                 angle_mode=0, device=0, use_graph=1, autotune=1, ordering=T.ORDER_AUTO):
         self.buses = np.ascontiguousarray(buses, dtype=T.BUS_DTYPE)
         self.branches = np.ascontiguousarray(branches, dtype=T.BRANCH_DTYPE)
         opt = T.Options()
         lib().mpf_default_options(ctypes.byref(opt))
         opt.max_it_nr, opt.max_it_fd, opt.tol = max_it_nr, max_it_fd, tol
         opt.angle_mode, opt.device, opt.use_graph, opt.autotune = angle_mode, device, use_graph, autotune
+        opt.ordering = ordering
         h = ctypes.c_void_p()
         rc = lib().mpf_create(ptr(self.buses), len(self.buses), ptr(self.branches), len(self.branches),
                               ctypes.byref(opt), ctypes.byref(h))

@@ -117,6 +117,7 @@ int main(int argc, char** argv) {
   const int nb = argc > 1 ? atoi(argv[1]) : 300;
   const int nbr = argc > 2 ? atoi(argv[2]) : 411;
   const int npv = argc > 3 ? atoi(argv[3]) : 69;
+  const int ordering = argc > 4 ? atoi(argv[4]) : 0;  // MPF_ORDER_*
   mpf_synth_params p;
   mpf_synth_default(&p);
   p.n_bus = nb;
@@ -127,7 +128,7 @@ int main(int argc, char** argv) {
   std::vector<mpf_branch> br(nbr);
   if (mpf_synth_grid(&p, b.data(), br.data()) != MPF_OK) return 2;
   GridSymbolic g;
-  if (!build_symbolic(b.data(), nb, br.data(), nbr, g).empty()) return 3;
+  if (!build_symbolic(b.data(), nb, br.data(), nbr, g, nullptr, ordering).empty()) return 3;
   Rng rng(11);
   // Newton system pattern, as the J fill scatters it (jpos)
   std::vector<int> rows, cols, aidx;

@@ -28,7 +28,7 @@ def test_library_exports_every_declared_entry_point():
     L = lib()
     missing = [d for d in declared if not hasattr(L, d)]
     assert not missing, missing
-    assert L.mpf_abi_version() == 2
+    assert L.mpf_abi_version() == 3
 
 
 def test_generator_is_deterministic_and_pinned():
@@ -106,10 +106,11 @@ def test_multifrontal_symbolic_by_host_emulation(tmp_path):
                     os.path.join(ROOT, "tests", "native", "mf_emulate.cpp"), os.path.join(csrc, "symbolic.cpp"),
                     os.path.join(csrc, "synth.cpp"), "-o", str(exe)], check=True, env=env)
     for args in (["30", "41", "5"], ["300", "411", "69"], ["2869", "4582", "509"]):
-        out = subprocess.run([str(exe)] + args, capture_output=True, text=True)
-        assert out.returncode == 0, out.stdout + out.stderr
-        errs = [float(x) for x in out.stdout.split()]
-        assert max(errs) < 1e-10
+        for ordering in ("0", "1", "2", "3"):  # automatic, minimum degree, minimum fill, weighted
+            out = subprocess.run([str(exe)] + args + [ordering], capture_output=True, text=True)
+            assert out.returncode == 0, out.stdout + out.stderr
+            errs = [float(x) for x in out.stdout.split()]
+            assert max(errs) < 1e-10
 
 
 def test_python_binding_reports_no_device_without_gpu():
