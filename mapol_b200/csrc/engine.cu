@@ -91,6 +91,11 @@ constexpr size_t kSmemMax = 227 * 1024;
 constexpr int kMaxQRounds = 20;
 // largest front any task class can hold: one FP64 lane, f * ((f + 1) | 1) * 8 bytes
 constexpr int kFmaxAll = 167;
+// backward solve: levels nearest the root with at most this many supernodes can run as
+// one k_mf_bsolve_top launch (an autotuner choice); codes kTopCode + G in the tuned
+// per-launch choices mark the launches it replaces
+constexpr int kTopLevelSn = 24;
+constexpr int kTopCode = 100;
 
 struct Launch {
   int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
@@ -179,6 +184,11 @@ struct LUSystem {
   // supernodes' parents
   std::vector<Launch> bsolve_sched;
   std::vector<LaunchDeps> bsolve_deps;
+  // the levels nearest the root, which k_mf_bsolve_top can solve in one launch:
+  // bsolve_sched[bs_top_from ..] are their launches; top_sn / top_lev_ptr list their
+  // supernodes from the root down, level by level
+  int bs_top_from = 0, top_nlev = 0, top_fcap = 0;
+  DevBuf top_sn, top_lev_ptr;
   std::unique_ptr<SideStreams> side = std::make_unique<SideStreams>();
   // autotuned kernel of every factor_sched launch, per (precision, case groups)
   uint64_t fingerprint = 0;          // of the symbolic structure (process-wide tuning cache key)
@@ -293,6 +303,28 @@ struct LUSystem {
     for (Launch& ln : bsolve_sched)
       for (int t = ln.offset; t < ln.offset + ln.count; ++t)
         ln.wfmax = std::max(ln.wfmax, s.sn_w[s.lev_sn[t]] * s.sn_f[s.lev_sn[t]]);
+    {
+      // near-root levels: from the root down while a level holds at most kTopLevelSn
+      // supernodes (too few to fill the GPU as a launch of its own)
+      int lcut = s.nlevels;
+      while (lcut > 0 && s.lev_ptr[lcut] - s.lev_ptr[lcut - 1] <= kTopLevelSn) --lcut;
+      bs_top_from = (int)bsolve_sched.size();
+      while (bs_top_from > 0 && bsolve_sched[bs_top_from - 1].level >= lcut) --bs_top_from;
+      std::vector<int> tsn, tlp{0};
+      top_fcap = 0;
+      for (int l = s.nlevels - 1; l >= lcut; --l) {
+        for (int k = s.lev_ptr[l]; k < s.lev_ptr[l + 1]; ++k) {
+          tsn.push_back(s.lev_sn[k]);
+          top_fcap = std::max(top_fcap, s.sn_f[s.lev_sn[k]]);
+        }
+        tlp.push_back((int)tsn.size());
+      }
+      top_nlev = s.nlevels - lcut;
+      if (top_nlev > 0) {
+        upload(top_sn, tsn);
+        upload(top_lev_ptr, tlp);
+      }
+    }
     bsolve_deps.assign(bsolve_sched.size(), LaunchDeps{});
     {
       std::vector<int> launch_of(s.nsn, -1);
@@ -447,6 +479,10 @@ void ensure_attrs(int device) {
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_fsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   done[device] = true;
 }
 
@@ -898,6 +934,25 @@ void launch_bsolve_one(int ge, const LUSystem& sys, const Launch& ln, int ngroup
   CUDA_TRY(cudaGetLastError());
 }
 
+// the near-root levels in one launch (k_mf_bsolve_top), a block per chunk of ge lanes
+template <typename T>
+void launch_bsolve_top(int ge, const LUSystem& sys, int ngroups, const T* pan, T* x, const int* group_active,
+                       cudaStream_t st) {
+  const DevLU dl = sys.dev();
+  const unsigned blocks = (unsigned)(ngroups * (32 / ge));
+  const size_t smem = (size_t)32 * sys.top_fcap * ge * sizeof(T);
+  const int* ts = sys.top_sn.as<int>();
+  const int* lp = sys.top_lev_ptr.as<int>();
+  switch (ge) {
+    case 8: k_mf_bsolve_top<T, 8><<<blocks, 1024, smem, st>>>(dl, ts, lp, sys.top_nlev, ngroups, sys.top_fcap, pan, x, group_active); break;
+    case 4: k_mf_bsolve_top<T, 4><<<blocks, 1024, smem, st>>>(dl, ts, lp, sys.top_nlev, ngroups, sys.top_fcap, pan, x, group_active); break;
+    case 2: k_mf_bsolve_top<T, 2><<<blocks, 1024, smem, st>>>(dl, ts, lp, sys.top_nlev, ngroups, sys.top_fcap, pan, x, group_active); break;
+    case 1: k_mf_bsolve_top<T, 1><<<blocks, 1024, smem, st>>>(dl, ts, lp, sys.top_nlev, ngroups, sys.top_fcap, pan, x, group_active); break;
+    default: throw MpfError{MPF_ERR_INTERNAL, "no near-root backward-solve kernel for this lane count"};
+  }
+  CUDA_TRY(cudaGetLastError());
+}
+
 // the fixed rule: one case per thread for small fronts; on levels with few
 // supernodes, fewer lanes per warp (more warps, more slots per lane)
 template <typename T>
@@ -928,8 +983,27 @@ void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const i
   cudaStream_t streams[4] = {st, ss.s[0], ss.s[1], ss.s[2]};
   int last[4] = {-1, -1, -1, -1};
   bool forked[4] = {true, false, false, false};
+  // the near-root levels as one launch when the tuner chose it (and no kernel is forced):
+  // it runs first on the caller's stream, and the events of the launches it replaces are
+  // recorded after it, so launches waiting for them wait for it
+  // MPF_BSOLVE_TOP (testing): run the near-root levels as one launch with this lane
+  // count (8, 4, 2, 1) whatever the tuner chose
+  int top_ge = 0;
+  if (it != sys.tuned_bs.end() && force == INT_MIN && sys.bs_top_from < n && it->second[n - 1] >= kTopCode)
+    top_ge = it->second[n - 1] - kTopCode;
+  if (const char* e = std::getenv("MPF_BSOLVE_TOP")) {
+    const int v = std::atoi(e);
+    if ((v == 8 || v == 4 || v == 2 || v == 1) && sys.top_nlev > 0) top_ge = v;
+  }
+  int kfrom = n - 1;
+  if (top_ge > 0) {
+    launch_bsolve_top<T>(top_ge, sys, ngroups, pan, x, group_active, st);
+    ++*nlaunch;
+    for (int k = sys.bs_top_from; k < n; ++k) CUDA_TRY(cudaEventRecord(ss.done[k], st));
+    kfrom = sys.bs_top_from - 1;
+  }
   CUDA_TRY(cudaEventRecord(ss.fork, st));
-  for (int k = n - 1; k >= 0; --k) {
+  for (int k = kfrom; k >= 0; --k) {
     const Launch& ln = sys.bsolve_sched[k];
     const LaunchDeps& dp = sys.bsolve_deps[k];
     cudaStream_t s = streams[dp.stream];
@@ -939,6 +1013,7 @@ void launch_bsolve(const LUSystem& sys, int ngroups, const T* pan, T* x, const i
     }
     for (int j : dp.wait) CUDA_TRY(cudaStreamWaitEvent(s, ss.done[j], 0));
     int ge = it != sys.tuned_bs.end() ? it->second[k] : bsolve_heuristic<T>(ln, ngroups);
+    if (ge >= kTopCode) ge -= kTopCode;  // a fused launch's level run on its own: the same chunk solve
     if (force != INT_MIN && (force >= 0 || bsolve_staged_smem(ln, -force, sizeof(T)) <= kSmemMax)) ge = force;
     launch_bsolve_one<T>(ge, sys, ln, ngroups, pan, x, group_active, s);
     ++*nlaunch;
@@ -967,7 +1042,11 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
         const int ge = it->second[k];
         ok = ge == 0 || ge == 16 || ge == 8 || ge == 4 || ge == 2 || ge == 1 ||
              ((ge == -8 || ge == -4 || ge == -2 || ge == -1) &&
-              bsolve_staged_smem(sys.bsolve_sched[k], -ge, sizeof(T)) <= kSmemMax);
+              bsolve_staged_smem(sys.bsolve_sched[k], -ge, sizeof(T)) <= kSmemMax) ||
+             // the fused near-root launch: the same code on every launch it replaces
+             ((ge == kTopCode + 8 || ge == kTopCode + 4 || ge == kTopCode + 2 || ge == kTopCode + 1) &&
+              (int)k >= sys.bs_top_from && ge == it->second.back());
+        if ((int)k >= sys.bs_top_from && (it->second.back() >= kTopCode) != (ge >= kTopCode)) ok = false;
       }
       if (ok) {
         sys.tuned_bs[{Prec<T>::idx, ngroups}] = it->second;
@@ -1025,6 +1104,45 @@ void tune_bsolve(LUSystem& sys, int ngroups, const T* pan, T* x, const int* grou
                      "best %.1f us (lanes %d), %.1f MB, %.0f GB/s\n", sys.sym.n, (int)sizeof(T) * 8, ngroups, k,
                      ln.count, ln.fcap, ht * 1e3, bt * 1e3, best[k], bytes * 1e-6, bytes / (bt * 1e-3) * 1e-9);
       }
+    }
+    // the near-root levels in one launch, against their tuned launches: the whole
+    // backward solve (launch DAG included, where those launches overlap) timed both ways
+    if (sys.top_nlev > 1 && (size_t)sys.top_fcap * 32 * 8 * sizeof(T) <= kSmemMax) {
+      const auto key2 = std::make_pair(Prec<T>::idx, ngroups);
+      auto whole = [&](const std::vector<int>& choice) {
+        sys.tuned_bs[key2] = choice;
+        int nl = 0;
+        float best_ms = 0.0f;
+        for (int rep = 0; rep < 3; ++rep) {
+          CUDA_TRY(cudaEventRecord(e0, st));
+          launch_bsolve<T>(sys, ngroups, pan, x, group_active, st, &nl);
+          CUDA_TRY(cudaEventRecord(e1, st));
+          CUDA_TRY(cudaEventSynchronize(e1));
+          float ms = 0.0f;
+          CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+          if (rep == 1 || (rep > 1 && ms < best_ms)) best_ms = ms;
+        }
+        return best_ms;
+      };
+      const float t_dag = whole(best);
+      int best_ge = 0;
+      float best_t = t_dag;
+      for (int ge : {8, 4, 2, 1}) {
+        std::vector<int> c = best;
+        for (int k = sys.bs_top_from; k < (int)c.size(); ++k) c[k] = kTopCode + ge;
+        const float t = whole(c);
+        if (t < best_t) {
+          best_t = t;
+          best_ge = ge;
+        }
+      }
+      sys.tuned_bs.erase(key2);
+      if (log)
+        std::fprintf(stderr, "mpf tune: n %d fp%d groups %d backward solve %.3f ms with %d near-root levels as %d "
+                     "launches, %.3f ms as one launch (lanes %d)\n", sys.sym.n, (int)sizeof(T) * 8, ngroups, t_dag,
+                     sys.top_nlev, (int)sys.bsolve_sched.size() - sys.bs_top_from, best_t, best_ge);
+      if (best_ge > 0)
+        for (int k = sys.bs_top_from; k < (int)sys.bsolve_sched.size(); ++k) best[k] = kTopCode + best_ge;
     }
     if (log)
       std::fprintf(stderr, "mpf tune: n %d fp%d groups %d backward solve heuristic %.3f ms, tuned %.3f ms\n",
@@ -1278,7 +1396,7 @@ struct mpf_handle {
       for (int p = 0; p < 2; ++p) b += s->A[p].bytes + s->pan[p].bytes + s->cb[p].bytes + s->cbr[p].bytes + s->x[p].bytes;
       const DevBuf* idx[] = {&s->sn_w, &s->sn_f, &s->sn_rptr, &s->sn_rows, &s->child_ptr, &s->child_list,
                              &s->sn_parent, &s->rel_ptr, &s->relmap, &s->ah_ptr, &s->ah_loc, &s->pan_off,
-                             &s->cb_off, &s->cbr_off, &s->lev_sn};
+                             &s->cb_off, &s->cbr_off, &s->lev_sn, &s->top_sn, &s->top_lev_ptr};
       for (auto q : idx) b += q->bytes;
     }
     for (int v = 0; v < 2; ++v) b += fdp[v].base.bytes + fdp[v].br_apos.bytes + fdp[v].br_bval.bytes +

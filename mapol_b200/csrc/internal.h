@@ -112,8 +112,10 @@ std::vector<int> minimum_degree(int n, const std::vector<std::vector<int>>& adj)
 // Minimum-deficiency (minimum fill-in) ordering: eliminates next the vertex whose
 // elimination adds the fewest edges among its neighbours, each missing edge (a, b)
 // counted weight[a] x weight[b] (weight null: 1).  Ties: smaller weighted degree,
-// then lowest index.  Returns perm as minimum_degree.
-std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj, const std::vector<int>* weight);
+// then lowest index.  Returns perm as minimum_degree, or an empty vector once the work
+// of counting fill (which grows with it) passes max_work (0: no limit).
+std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj, const std::vector<int>* weight,
+                              long long max_work = 0);
 
 // Everything that does not depend on the case batch.
 struct GridSymbolic {

@@ -1180,6 +1180,55 @@ __global__ void __launch_bounds__(128) k_mf_bsolve_chunk(DevLU L, const int* __r
   }
 }
 
+// Backward substitution of the levels nearest the root in one launch.  A block per
+// chunk of G lanes walks those levels from the root down; the block's warps take the
+// supernodes of a level (as k_mf_bsolve_chunk: 32 / G slots per lane split each pivot
+// row's dot product, folded with shuffles), and a block barrier separates the levels,
+// so every parent is solved before its children read its x.  Lanes are independent:
+// blocks never wait on each other, and one launch replaces the launches of those
+// levels (each of which had too few supernodes to fill the GPU) and the gaps between
+// them.  32 warps per block: a level's supernodes (at most 24) take one round.
+// top_sn: the supernodes of those levels in descending level order, lev_ptr[l]
+// .. lev_ptr[l + 1] the ones of the l-th level from the top; fcap: their largest front.
+template <typename T, int G>
+__global__ void __launch_bounds__(1024) k_mf_bsolve_top(DevLU L, const int* __restrict__ top_sn,
+                                                       const int* __restrict__ lev_ptr, int nlev, int ngroups, int fcap,
+                                                       const T* __restrict__ pan, T* __restrict__ x,
+                                                       const int* __restrict__ group_active) {
+  constexpr int SLOTS = 32 / G, LPG = 32 / G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  const int slot = tid / G, l = tid % G;
+  T* xs = reinterpret_cast<T*>(smem_raw) + (size_t)warp * fcap * G;
+  const int ch = blockIdx.x;
+  const int g = ch / LPG;
+  if (g >= ngroups || !group_active[g]) return;  // uniform over the block, before any barrier
+  const int lane = (ch % LPG) * G + l;
+  for (int lv = 0; lv < nlev; ++lv) {
+    for (int k = lev_ptr[lv] + warp; k < lev_ptr[lv + 1]; k += warps) {
+      const int s = top_sn[k];
+      if (!task_here(L, s, g)) continue;
+      const int w = L.sn_w[s], f = L.sn_f[s];
+      const int* rows = L.sn_rows + L.sn_rptr[s];
+      const long long po = L.pan_off[s];
+      for (int q = slot; q < f; q += SLOTS) xs[q * G + l] = x[at32(g, L.n, rows[q], lane)];
+      __syncwarp();
+      for (int p = w - 1; p >= 0; --p) {
+        const T* urow = pan + at32(g, L.nnz, po + (long long)p * f, lane);
+        T part = (T)0;
+        for (int q = p + 1 + slot; q < f; q += SLOTS) part += urow[(size_t)q * 32] * xs[q * G + l];
+#pragma unroll
+        for (int o = 16; o >= G; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (slot == 0) xs[p * G + l] = (xs[p * G + l] - part) / urow[(size_t)p * 32];
+        __syncwarp();
+      }
+      for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, rows[p], lane)] = xs[p * G + l];
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+}
+
 // Backward substitution with the U panel staged in shared memory: one warp per
 // (supernode, chunk of G lanes) copies the supernode's whole U panel (w x f entries
 // of its G lanes) and the front's x values into shared memory with asynchronous

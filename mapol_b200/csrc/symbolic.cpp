@@ -12,6 +12,8 @@
 //    symbolic LU and base values.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <set>
@@ -82,7 +84,8 @@ std::vector<int> minimum_degree(int n, const std::vector<std::vector<int>>& adj0
   return perm;
 }
 
-std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj0, const std::vector<int>* weight) {
+std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj0, const std::vector<int>* weight,
+                              long long max_work) {
   std::vector<std::vector<int>> adj(n);
   for (int v = 0; v < n; ++v)
     for (int a : adj0[v])
@@ -97,6 +100,7 @@ std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj0, 
   auto W = [&](int v) -> long long { return weight ? (*weight)[v] : 1; };
   std::vector<int> mark(n, -1);
   int stamp = 0;
+  long long work = 0;  // inner steps of the fill counts (their cost grows with the fill)
   // weighted count of the edges that eliminating v would add (pairs of its
   // neighbours not yet adjacent)
   auto fill_of = [&](int v) {
@@ -105,6 +109,7 @@ std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj0, 
     for (size_t i = 0; i + 1 < nb.size(); ++i) {
       ++stamp;
       for (int x : adj[nb[i]]) mark[x] = stamp;
+      work += (long long)adj[nb[i]].size() + (long long)(nb.size() - i);
       for (size_t j = i + 1; j < nb.size(); ++j)
         if (mark[nb[j]] != stamp) f += W(nb[i]) * W(nb[j]);
     }
@@ -161,7 +166,9 @@ std::vector<int> minimum_fill(int n, const std::vector<std::vector<int>>& adj0, 
       deg[u] = degree_of(u);
       pq.insert({fill[u], deg[u], u});
     }
+    if (max_work > 0 && work > max_work) return {};  // too dense for this method
   }
+  if (const char* e = std::getenv("MPF_ORDER_WORK_LOG")) std::fprintf(stderr, "minimum_fill work %lld\n", work);
   return perm;
 }
 
@@ -692,9 +699,13 @@ std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, i
   // (factorisation + backward solve = 3.24 ms per MFLOP per case + 0.172 ms per level).
   std::vector<int> wvar(nfree);
   for (int a = 0; a < nfree; ++a) wvar[a] = has_vm(free_bus[a]) ? 2 : 1;
-  auto order_of = [&](int method) {
-    if (method == MPF_ORDER_MIN_FILL) return minimum_fill(nfree, badj, nullptr);
-    if (method == MPF_ORDER_MIN_FILL_WEIGHTED) return minimum_fill(nfree, badj, &wvar);
+  // budget of the automatic choice's minimum-fill runs: their cost grows with the fill,
+  // so on densely meshed grids (where fronts are large anyway) they give way to
+  // minimum degree; a method asked for explicitly always runs
+  const long long work_cap = 400LL * 1000 * 1000;
+  auto order_of = [&](int method, long long cap) {
+    if (method == MPF_ORDER_MIN_FILL) return minimum_fill(nfree, badj, nullptr, cap);
+    if (method == MPF_ORDER_MIN_FILL_WEIGHTED) return minimum_fill(nfree, badj, &wvar, cap);
     return minimum_degree(nfree, badj);
   };
   int method = ordering;
@@ -702,7 +713,9 @@ std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, i
     constexpr double kLevelFlops = 53000.0;
     double best = 0.0;
     for (int m : {MPF_ORDER_MIN_DEGREE, MPF_ORDER_MIN_FILL, MPF_ORDER_MIN_FILL_WEIGHTED}) {
-      newton_symbolic(order_of(m));
+      const std::vector<int> ord = order_of(m, work_cap);
+      if (ord.empty()) continue;
+      newton_symbolic(ord);
       const double cost = (double)g.jac.flops + kLevelFlops * g.jac.nlevels;
       if (method == MPF_ORDER_AUTO || cost < best) {
         best = cost;
@@ -710,7 +723,7 @@ std::string build_symbolic(const mpf_bus* buses, int nb, const mpf_branch* br, i
       }
     }
   }
-  newton_symbolic(order_of(method));
+  newton_symbolic(order_of(method, 0));
   g.ordering = method;
   // J entries: the (Va,Va), (Va,Vm), (Vm,Va), (Vm,Vm) quadrants of every Ybus entry
   // between PV/PQ buses (newtonpf.h:215-295 enumerate the same set)

@@ -5,7 +5,10 @@ run may use any of them.  MPF_BSOLVE_LANES forces one kernel on every level: the
 one-case-per-thread kernel (0), k_mf_bsolve_chunk<G> (G) or k_mf_bsolve_staged<G>
 (-G).  Each must converge to the oracle's voltages (1e-8 p.u., as the parity tests)
 with the oracle's iteration counts, and the staged kernel, which sums in another
-order, must agree with the chunk kernel to round-off.
+order, must agree with the chunk kernel to round-off.  MPF_BSOLVE_TOP forces the
+near-root levels into one k_mf_bsolve_top launch, which does the chunk kernel's
+arithmetic: with the other levels on the chunk kernel of the same lane count, the
+results must be the same bit for bit.
 """
 import os
 
@@ -18,8 +21,10 @@ from oracle import oracle
 pytestmark = pytest.mark.gpu
 
 
-def _solve(buses, branches, cases, prec, lanes):
+def _solve(buses, branches, cases, prec, lanes, top=None):
     os.environ["MPF_BSOLVE_LANES"] = str(lanes)
+    if top:
+        os.environ["MPF_BSOLVE_TOP"] = str(top)
     try:
         with m.PowerFlow(buses, branches) as pf:
             pf.set_cases(cases)
@@ -27,6 +32,7 @@ def _solve(buses, branches, cases, prec, lanes):
             return pf.results()
     finally:
         del os.environ["MPF_BSOLVE_LANES"]
+        os.environ.pop("MPF_BSOLVE_TOP", None)
 
 
 @pytest.mark.parametrize("prec", [m.MIXED, m.FP64])
@@ -56,3 +62,19 @@ def test_forced_kernels_match_oracle(gpu):
         assert np.array_equal(conv, ref["converged"])
         assert np.array_equal(res.iterations[conv], ref["iterations"][conv]), lanes
         assert np.abs(res.v[conv] - ref["v"][conv]).max() < 1e-8, lanes
+
+
+@pytest.mark.parametrize("prec", [m.MIXED, m.FP64])
+def test_fused_near_root_levels_equal_chunk_kernel(gpu, prec):
+    buses, branches, cases = m.workload("cfg3_9241bus")
+    cases = cases[:96]
+    ref = oracle.runpf(buses, branches, cases[:16], alg=m.NR)
+    for g in (8, 4, 2, 1):
+        a = _solve(buses, branches, cases, prec, g)
+        b = _solve(buses, branches, cases, prec, g, top=g)
+        assert np.array_equal(a.status, b.status) and np.array_equal(a.iterations, b.iterations)
+        assert np.array_equal(a.v, b.v), g
+        conv = b.status[:16] == m.runpf.CONVERGED
+        assert np.array_equal(conv, ref["converged"])
+        if prec == m.FP64:  # (mixed precision: the parity tests' rules, bitwise equality here)
+            assert np.abs(b.v[:16][conv] - ref["v"][conv]).max() < 1e-8
