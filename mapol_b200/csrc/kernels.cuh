@@ -557,6 +557,16 @@ template <typename T, int V>
 __device__ __forceinline__ Lanes<T, V> ld(const T* p) { return *reinterpret_cast<const Lanes<T, V>*>(p); }
 template <typename T, int V>
 __device__ __forceinline__ void st(T* p, const Lanes<T, V>& a) { *reinterpret_cast<Lanes<T, V>*>(p) = a; }
+// V adjacent lanes of one entry copied global -> shared asynchronously (cp.async, cache
+// at all levels); both addresses aligned to the copy size; completes at the next
+// cp.async.wait_all of the issuing thread
+template <typename T, int V>
+__device__ __forceinline__ void cp_async(T* dst_shared, const T* src_global) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst_shared);
+  constexpr int B = V * (int)sizeof(T);
+  static_assert(B == 4 || B == 8 || B == 16, "cp.async moves 4, 8 or 16 bytes");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(src_global), "n"(B) : "memory");
+}
 
 // Partial LU of a front held in registers (256 threads as 16 x 16; thread (r, c)
 // owns entries (r + 16 a, c + 16 b), a, b < TT, of its V lanes).  Per pivot the
@@ -725,25 +735,24 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
     }
     team_sync<TEAM>();
     {
+      // the arrowhead values (and the pivot rows' right-hand side) are assignments into
+      // the zeroed front: asynchronous global-to-shared copies put all of a task's in
+      // flight at once without holding registers, then one wait
       const T* a0 = A + at32(g, L.nA, 0, lane);
-      // four entries' index and value loads in flight before their stores
       const int e1 = ah1;
       int e = ah0 + slot;
-      for (; e + 3 * SLOTS < e1; e += 4 * SLOTS) {
-        int loc[4];
-        LV v[4];
+      for (; e + 7 * SLOTS < e1; e += 8 * SLOTS) {
+        int loc[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          loc[u] = L.ah_loc[e + u * SLOTS];
-          v[u] = ld<T, V>(a0 + (size_t)(e + u * SLOTS) * 32);
-        }
+        for (int u = 0; u < 8; ++u) loc[u] = L.ah_loc[e + u * SLOTS];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) st<T, V>(F + loc[u] * G, v[u]);
+        for (int u = 0; u < 8; ++u) cp_async<T, V>(F + loc[u] * G, a0 + (size_t)(e + u * SLOTS) * 32);
       }
-      for (; e < e1; e += SLOTS) st<T, V>(F + L.ah_loc[e] * G, ld<T, V>(a0 + (size_t)e * 32));
+      for (; e < e1; e += SLOTS) cp_async<T, V>(F + L.ah_loc[e] * G, a0 + (size_t)e * 32);
+      if (with_rhs)
+        for (int p = slot; p < w; p += SLOTS) cp_async<T, V>(FP(p, f), x + at32(g, L.n, rows[p], lane));
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
     }
-    if (with_rhs)
-      for (int p = slot; p < w; p += SLOTS) st<T, V>(FP(p, f), ld<T, V>(x + at32(g, L.n, rows[p], lane)));
     team_sync<TEAM>();
     ChildRef next = ci0 < ci1 ? L.child_ref[ci0] : ChildRef{};
     for (int ci = ci0; ci < ci1; ++ci) {
