@@ -177,6 +177,47 @@ def cpu_port_baseline(buses, branches, cases, budget_s=15.0):
     return line, r
 
 
+def other_cpu_baselines(buses, branches, cases, budget_s=10.0):
+    """The other CPU rows, each on a bounded sample on all host threads: Newton with
+    the reference's Eigen SparseLU reusing its symbolic analysis within a case (the
+    reference calls compute(), i.e. analysis and factorisation, every iteration;
+    newtonpf.h:341-363), and fast-decoupled XB (fdpf.h:450-596) on the oracle's own LU."""
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    out = {}
+    if oracle.has_eigen():
+        # one and two iterations of one case per thread: their difference is a
+        # factorisation with the analysis reused, the first run the analysis and one
+        sample = cases[:threads]
+        t = time.perf_counter()
+        oracle.runpf(buses, branches, sample, max_it=1, solver=oracle.SOLVER_EIGEN_REUSE, threads=threads)
+        t1 = time.perf_counter() - t
+        t = time.perf_counter()
+        oracle.runpf(buses, branches, sample, max_it=2, solver=oracle.SOLVER_EIGEN_REUSE, threads=threads)
+        t2 = time.perf_counter() - t
+        iters = 7.0  # every case of the 9241-bus workload converges in 7 (oracle and engine)
+        per_solve = t1 + (iters - 1.0) * max(t2 - t1, 0.0)
+        out["newton_eigen_symbolic_reused"] = {
+            "value": len(sample) / per_solve, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} cases, one per thread: analysis + first iteration {t1:.1f} s, each further "
+                      f"iteration {t2 - t1:.1f} s; a 7-iteration solve = first + 6 further"}
+    n = min(len(cases), max(threads, 8))
+    t = time.perf_counter()
+    r = oracle.runpf(buses, branches, cases[:n], alg=1, threads=threads)
+    dt = time.perf_counter() - t
+    if dt < budget_s / 4 and n < len(cases):
+        n = min(len(cases), int(n * budget_s / max(dt, 1e-3)))
+        t = time.perf_counter()
+        r = oracle.runpf(buses, branches, cases[:n], alg=1, threads=threads)
+        dt = time.perf_counter() - t
+    out["fdxb_own_lu"] = {"value": n / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+                          "sample": f"{n} cases, fast-decoupled XB to 1e-8 on the oracle's sparse LU "
+                                    f"(B' and B'' refactorised every iteration, as fdpf.h:483-561), {dt:.1f} s",
+                          "converged": int(r["converged"].sum())}
+    return out
+
+
 def accuracy(res, ref):
     """Per-result accuracy of GPU results against the FP64 oracle on the cases both
     solved: max |dV| (p.u., complex difference), max angle error (degrees), flag and
@@ -506,6 +547,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if e2e:
         line["e2e"] = e2e
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baselines"] = other_cpu_baselines(buses, branches, cases)
     line["setup"] = {"mpf_create_ms": round(t_create * 1e3, 1),
                      "note": "one-time host symbolic analysis (ordering, supernodes, relative maps) and "
                              "upload of the shared arrays; not inside the timed solves"}

@@ -25,11 +25,12 @@
 // with compute() on every solve, exactly the reference's Eigen_SparseLU option
 // (newtonpf.h:341-363).
 //
-// Parity pin: the reference ships no tests, golden vectors or solved outputs, and
-// its own CPU path needs Intel MKL (absent here), so this oracle is "parity
-// unpinned" against reference outputs.  It is cross-checked instead against an
-// independent numpy/scipy polar-form Newton-Raphson, against hand-solvable 2-bus
-// cases, and (solver option) against the reference's own Eigen SparseLU.
+// Parity pin: the reference's own CPU power flow, compiled unmodified from its sources
+// into oracle/_ref/librefpf.so (oracle/ref_pf.cu, with in-project MKL stand-ins),
+// produces the same converged flags and iteration counts and voltages within ~1e-13 on
+// its bundled MATPOWER cases with N-1 outages, for NR, FDXB and FDBX
+// (tests/test_oracle_reference_pin.py).  Also cross-checked against an independent
+// numpy/scipy polar-form Newton-Raphson and hand-solvable 2-bus cases.
 //
 // Quirk policy (reference behaviours the oracle chooses explicitly):
 //   * convergence uses max |F| (CPU path, newtonpf.h:59-67), not the GPU path's
@@ -41,6 +42,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <set>
 #include <vector>
 
@@ -52,6 +54,7 @@
 
 #define ORACLE_SOLVER_GP 0
 #define ORACLE_SOLVER_EIGEN 1
+#define ORACLE_SOLVER_EIGEN_REUSE 2  // Eigen SparseLU, analyzePattern once per case, factorize per solve
 
 namespace {
 
@@ -425,8 +428,32 @@ struct SparseLUPP {
 struct Solver {
   int kind = ORACLE_SOLVER_GP;
   std::vector<int> order;  // cached column order for GP (pattern fixed per system)
+#ifdef ORACLE_WITH_EIGEN
+  // ORACLE_SOLVER_EIGEN_REUSE: the same SparseLU with its symbolic analysis (COLAMD
+  // ordering, elimination tree) done on the first solve and reused, the pattern of the
+  // system being fixed
+  std::unique_ptr<Eigen::SparseLU<Eigen::SparseMatrix<double>, Eigen::COLAMDOrdering<int> > > reuse;
+#endif
   bool solve(const CsrR& A, const std::vector<double>& b, std::vector<double>& x) {
 #ifdef ORACLE_WITH_EIGEN
+    if (kind == ORACLE_SOLVER_EIGEN_REUSE) {
+      Eigen::SparseMatrix<double> M(A.n, A.n);
+      for (int i = 0; i < A.n; ++i)
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) M.insert(i, A.col[k]) = A.val[k];
+      M.makeCompressed();
+      if (!reuse) {
+        reuse.reset(new Eigen::SparseLU<Eigen::SparseMatrix<double>, Eigen::COLAMDOrdering<int> >());
+        reuse->analyzePattern(M);
+      }
+      reuse->factorize(M);
+      if (reuse->info() != Eigen::Success) return false;
+      Eigen::VectorXd B(A.n);
+      for (int i = 0; i < A.n; ++i) B(i) = b[i];
+      Eigen::VectorXd X = reuse->solve(B);
+      x.assign(A.n, 0.0);
+      for (int i = 0; i < A.n; ++i) x[i] = X(i);
+      return true;
+    }
     if (kind == ORACLE_SOLVER_EIGEN) {
       // newtonpf.h:341-363: insert, makeCompressed, SparseLU<COLAMD>.compute, solve
       Eigen::SparseMatrix<double> M(A.n, A.n);
@@ -640,7 +667,7 @@ int oracle_runpf(const mpf_bus* buses, int nb, const mpf_branch* branches, int n
                  double* v_out, int* iters, unsigned char* converged, double* max_mis,
                  int n_threads) {
   if (!buses || !branches || nb < 2 || nbr < 1 || n_cases < 0) return -1;
-  if (solver == ORACLE_SOLVER_EIGEN && !oracle_has_eigen()) return -1;
+  if ((solver == ORACLE_SOLVER_EIGEN || solver == ORACLE_SOLVER_EIGEN_REUSE) && !oracle_has_eigen()) return -1;
   Grid g;
   g.nb = nb;
   g.nbr = nbr;

@@ -2,10 +2,14 @@
 only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm,
 always as the checker or as the timed CPU baseline.
 
-Parity pin status: the reference ships no tests, golden vectors or solved outputs
-and its CPU path needs Intel MKL (absent), so the oracle is "parity unpinned"
-against reference outputs; it is cross-checked against an independent numpy/scipy
-Newton-Raphson, analytic 2-bus cases, and the reference's own Eigen SparseLU.
+Parity pin: the oracle reproduces the reference's own CPU power flow (its runpf.h and
+the headers it includes, compiled unmodified into oracle/_ref/librefpf.so, see
+refpf.py): identical converged flags and iteration counts and voltages to ~1e-13 on
+the reference's bundled MATPOWER cases with N-1 outages (tests/test_oracle_reference_pin.py).
+It is also cross-checked against an independent numpy/scipy Newton-Raphson and
+analytic 2-bus cases.  Solvers: SOLVER_GP (own sparse LU, minimum degree),
+SOLVER_EIGEN (the reference's Eigen SparseLU option, compute() every solve),
+SOLVER_EIGEN_REUSE (the same with its symbolic analysis done once per case).
 """
 import ctypes
 import os
@@ -16,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_OWN = os.path.join(HERE, "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "liboracle.so")
 
-SOLVER_GP, SOLVER_EIGEN = 0, 1
+SOLVER_GP, SOLVER_EIGEN, SOLVER_EIGEN_REUSE = 0, 1, 2
 
 _libs = {}
 
@@ -46,7 +50,8 @@ def has_eigen():
 
 
 def _lib_for(solver):
-    return _load(LIB_REF if solver == SOLVER_EIGEN else (LIB_OWN if os.path.exists(LIB_OWN) else LIB_REF))
+    eigen = solver in (SOLVER_EIGEN, SOLVER_EIGEN_REUSE)
+    return _load(LIB_REF if eigen else (LIB_OWN if os.path.exists(LIB_OWN) else LIB_REF))
 
 
 def _p(a):
