@@ -96,6 +96,12 @@ constexpr int kFmaxAll = 167;
 // per-launch choices mark the launches it replaces
 constexpr int kTopLevelSn = 24;
 constexpr int kTopCode = 100;
+// factorisation launches split by front size (LUSystem::split_factor_launches; a ratio
+// of at most 1 keeps one launch per level and task class).  9241-bus workload, mixed /
+// FP64 solves/s: no split 35.7k / 22.5k, 1.35 with 64 supernodes 36.7k / 23.4k, 1.6
+// with 128 35.9k / 22.6k
+constexpr double kSplitRatio = 1.35;
+constexpr int kSplitMinSn = 64;
 
 struct Launch {
   int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
@@ -174,7 +180,7 @@ struct FactorChoice {
 struct LUSystem {
   LUSymbolic sym;
   DevBuf sn_w, sn_f, sn_rptr, sn_rows, child_ptr, child_list, sn_parent, rel_ptr, relmap, ah_ptr, ah_loc;
-  DevBuf pan_off, cb_off, cbr_off, lev_sn, child_ref;
+  DevBuf pan_off, cb_off, cbr_off, lev_sn, child_ref, cb_in;
   DevBuf sn_island;                  // multi-island handles only
   const int* group_island = nullptr; // the handle's current per-group islands (or null)
   std::vector<Launch> factor_sched;  // ascending levels
@@ -225,6 +231,7 @@ struct LUSystem {
     d.cb_off = cb_off.as<long long>();
     d.cbr_off = cbr_off.as<long long>();
     d.child_ref = child_ref.as<ChildRef>();
+    d.cb_in = cb_in.as<CbIn>();
     d.sn_island = group_island ? sn_island.as<int>() : nullptr;
     d.group_island = group_island;
     return d;
@@ -269,6 +276,21 @@ struct LUSystem {
       cr[q] = ChildRef{s.cb_off[c], s.cbr_off[c], s.sn_f[c] - s.sn_w[c], s.rel_ptr[c]};
     }
     upload(child_ref, cr);
+    std::vector<CbIn> ci(s.nsn, CbIn{0, 0, 0, 0});
+    for (int q = 0; q < s.nsn; ++q) {
+      if (s.child_ptr[q] == s.child_ptr[q + 1]) continue;
+      const int c0 = s.child_list[s.child_ptr[q]];
+      ci[q].cb = s.cb_off[c0];
+      ci[q].cbr = s.cbr_off[c0];
+      for (int c = s.child_ptr[q]; c < s.child_ptr[q + 1]; ++c) {
+        const int ch = s.child_list[c], m = s.sn_f[ch] - s.sn_w[ch];
+        if (s.cb_off[ch] != ci[q].cb + ci[q].ncb || s.cbr_off[ch] != ci[q].cbr + ci[q].ncbr)
+          throw MpfError{MPF_ERR_INTERNAL, "contribution blocks of siblings are not adjacent"};
+        ci[q].ncb += m * m;
+        ci[q].ncbr += m;
+      }
+    }
+    upload(cb_in, ci);
     fingerprint = structure_fingerprint(s);
     factor_sched.clear();
     level_sched.clear();
@@ -300,6 +322,11 @@ struct LUSystem {
     }
     // the backward substitution's launches and their DAG (top-down: parents first)
     bsolve_sched = factor_sched;
+    split_factor_launches(s);
+    for (const Launch& ln : factor_sched) {
+      fingerprint = (fingerprint ^ (uint64_t)ln.offset) * 1099511628211ull;
+      fingerprint = (fingerprint ^ (uint64_t)ln.count) * 1099511628211ull;
+    }
     for (Launch& ln : bsolve_sched)
       for (int t = ln.offset; t < ln.offset + ln.count; ++t)
         ln.wfmax = std::max(ln.wfmax, s.sn_w[s.lev_sn[t]] * s.sn_f[s.lev_sn[t]]);
@@ -372,6 +399,41 @@ struct LUSystem {
           }
       }
     }
+  }
+
+  // A launch's shared memory per team is set by its largest front, while its fronts'
+  // sizes spread (a level's supernodes are sorted by front size): a run of fronts
+  // 9..16 reserves 16 x 17 entries per lane for fronts averaging 12 x 13.  Shared
+  // memory bounds the resident teams, and the teams in flight bound these
+  // latency-bound launches, so a run splits where the next front would need more
+  // than kSplitRatio times the shared memory of the run's first front, as long as both
+  // parts keep at least kSplitMinSn supernodes (enough tasks to fill the GPU).
+  void split_factor_launches(const LUSymbolic& s) {
+    double ratio = kSplitRatio;
+    int min_sn = kSplitMinSn;
+    if (const char* e = std::getenv("MPF_FSPLIT")) ratio = std::atof(e);
+    if (const char* e = std::getenv("MPF_FSPLIT_MIN")) min_sn = std::max(1, std::atoi(e));
+    if (!(ratio > 1.0)) return;
+    auto area = [](int f) { return (double)f * front_stride(f); };
+    std::vector<Launch> out;
+    for (const Launch& ln : factor_sched) {
+      int k = ln.offset;
+      const int end = ln.offset + ln.count;
+      while (k < end) {
+        const int f0 = s.sn_f[s.lev_sn[k]];
+        int k2 = k + 1;
+        while (k2 < end && (area(s.sn_f[s.lev_sn[k2]]) <= ratio * area(f0) || k2 - k < min_sn)) ++k2;
+        if (end - k2 < min_sn) k2 = end;  // a short remainder joins this part
+        Launch p = ln;
+        p.offset = k;
+        p.count = k2 - k;
+        p.fcap = 0;
+        for (int q = k; q < k2; ++q) p.fcap = std::max(p.fcap, s.sn_f[s.lev_sn[q]]);
+        out.push_back(p);
+        k = k2;
+      }
+    }
+    factor_sched = out;
   }
 
   // Values one factorisation launch moves per case: arrowhead reads, children's
@@ -1396,7 +1458,8 @@ struct mpf_handle {
       for (int p = 0; p < 2; ++p) b += s->A[p].bytes + s->pan[p].bytes + s->cb[p].bytes + s->cbr[p].bytes + s->x[p].bytes;
       const DevBuf* idx[] = {&s->sn_w, &s->sn_f, &s->sn_rptr, &s->sn_rows, &s->child_ptr, &s->child_list,
                              &s->sn_parent, &s->rel_ptr, &s->relmap, &s->ah_ptr, &s->ah_loc, &s->pan_off,
-                             &s->cb_off, &s->cbr_off, &s->lev_sn, &s->top_sn, &s->top_lev_ptr};
+                             &s->cb_off, &s->cbr_off, &s->lev_sn, &s->top_sn, &s->top_lev_ptr,
+                             &s->child_ref, &s->cb_in};
       for (auto q : idx) b += q->bytes;
     }
     for (int v = 0; v < 2; ++v) b += fdp[v].base.bytes + fdp[v].br_apos.bytes + fdp[v].br_bval.bytes +

@@ -62,8 +62,10 @@ struct LUSymbolic {
   std::vector<int> lev_ptr, lev_sn;  // supernodes grouped by level, by front size within a level
   std::vector<int> child_ptr, child_list;
   std::vector<int64_t> pan_off;      // nsn+1, entries
-  std::vector<int64_t> cb_off;       // nsn+1, (f-w)^2 per supernode
-  std::vector<int64_t> cbr_off;      // nsn+1, (f-w) per supernode
+  // offsets of each supernode's contribution block ((f-w)^2 entries) and carried
+  // right-hand side (f-w); siblings adjacent; [nsn] = the totals
+  std::vector<int64_t> cb_off;       // nsn+1
+  std::vector<int64_t> cbr_off;      // nsn+1
   std::vector<int> rel_ptr, relmap;  // per supernode: CB index -> index in the parent's front
   std::vector<int> sn_of;            // per variable
   int max_front = 0;

@@ -113,6 +113,13 @@ struct ChildRef {
   long long cb_off, cbr_off;
   int m, rel_ptr;
 };
+// Everything a supernode assembles from its children: the children's contribution
+// blocks (entries [cb, cb + ncb)) and carried right-hand sides ([cbr, cbr + ncbr)),
+// adjacent in storage
+struct CbIn {
+  long long cb, cbr;
+  int ncb, ncbr;
+};
 
 struct DevLU {
   int n, nsn, nA;
@@ -124,6 +131,7 @@ struct DevLU {
   const int* child_ptr;
   const int* child_list;
   const ChildRef* child_ref;  // per child_list position
+  const CbIn* cb_in;          // per supernode
   const int* sn_parent;
   const int* rel_ptr;
   const int* relmap;
@@ -568,6 +576,12 @@ __device__ __forceinline__ void cp_async(T* dst_shared, const T* src_global) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(src_global), "n"(B) : "memory");
 }
 
+// Asks L2 to fetch [p, p + bytes) from DRAM (bulk prefetch: no completion, no data
+// returned to the thread); p and bytes multiples of 16
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Partial LU of a front held in registers (256 threads as 16 x 16; thread (r, c)
 // owns entries (r + 16 a, c + 16 b), a, b < TT, of its V lanes).  Per pivot the
 // owners publish column p (rows >= p) and row p (columns > p) to a shared buffer
@@ -683,8 +697,13 @@ __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int
 // TT > 0: the partial LU runs in registers (lu_registers; TEAM 256 with one thread
 // per entry-lane group, i.e. G <= 16 bytes of lanes); TT = 0: in shared memory, one
 // barrier per pivot; TT = -2: in shared memory, two pivots per barrier.
+//
+// Register budgets: warp teams are launched in blocks of at most 256 threads; their
+// bound of 288 threads x 3 blocks gives them 72 registers (no spills; shared memory
+// holds them to at most ~24 warps per SM anyway).  9241-bus workload, mixed solves/s
+// at 64 / 72 / 80 registers: 34.7k / 35.7k / 35.8k (64 spills 48 bytes per thread).
 template <typename T, int G, int TEAM, int TT = 0>
-__global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 256 ? 1 : (TT < 0 ? 2 : 4))) k_mf_factor(
+__global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 1 : (TEAM > 256 ? 1 : (TT < 0 ? 2 : (TEAM == 32 ? 3 : 4)))) k_mf_factor(
     DevLU L, const int* __restrict__ task_sn, int nsn_l, int ngroups, int fcap,
     const T* __restrict__ A, T* __restrict__ pan, T* __restrict__ cb, T* __restrict__ cbr,
     T* __restrict__ x, int* __restrict__ status, const int* __restrict__ group_active, int with_rhs) {
@@ -725,6 +744,19 @@ __global__ void __launch_bounds__(TEAM == 32 ? 256 : TEAM, TT > 0 ? 1 : (TEAM > 
     const long long cbo_s = L.cb_off[s], cbro_s = L.cbr_off[s];
     const int RS = front_stride(f);
     const int ncols = with_rhs ? f + 1 : f;
+    // The task's global inputs are two or three contiguous blocks per group of 32 lanes:
+    // its arrowhead values, its children's contribution blocks and their carried
+    // right-hand sides (siblings are adjacent in storage).  Bulk L2 prefetches of these,
+    // issued before the front is zeroed, start all of the task's DRAM reads at once; the
+    // loads of the assembly then mostly wait on L2.  The other lane chunks of a group
+    // ask for the same lines, which L2 merges.
+    {
+      const CbIn cin = L.cb_in[s];
+      constexpr unsigned B32 = 32 * sizeof(T);  // one entry of a group
+      if (tid == 0 && ah1 > ah0) prefetch_l2(A + at32(g, L.nA, ah0, 0), (unsigned)(ah1 - ah0) * B32);
+      if (tid == 1 && cin.ncb > 0) prefetch_l2(cb + at32(g, L.sumcb, cin.cb, 0), (unsigned)cin.ncb * B32);
+      if (tid == 2 && with_rhs && cin.ncbr > 0) prefetch_l2(cbr + at32(g, L.sumcbr, cin.cbr, 0), (unsigned)cin.ncbr * B32);
+    }
     // F + (r * RS + c) * G: entry (r, c) of this thread's lanes
 #define FP(r, c) (F + ((r) * RS + (c)) * G)
     {

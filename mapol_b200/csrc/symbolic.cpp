@@ -367,6 +367,25 @@ void lu_symbolic(int n, const std::vector<std::vector<int>>& adj, LUSymbolic& s,
     }
     s.sum_cb += (int64_t)(f - w) * (f - w);
   }
+  // contribution blocks are stored parent by parent, the children of a supernode
+  // adjacent in child_list order, so that everything a front assembles from its
+  // children is one contiguous range (cb_off[nsn] / cbr_off[nsn] stay the totals)
+  {
+    int64_t off = 0, roff = 0;
+    auto place = [&](int q) {
+      const int64_t m = s.sn_f[q] - s.sn_w[q];
+      s.cb_off[q] = off;
+      s.cbr_off[q] = roff;
+      off += m * m;
+      roff += m;
+    };
+    for (int q = 0; q < ns; ++q)
+      for (int c = s.child_ptr[q]; c < s.child_ptr[q + 1]; ++c) place(s.child_list[c]);
+    for (int q = 0; q < ns; ++q)
+      if (s.sn_parent[q] < 0) place(q);
+    s.cb_off[ns] = off;
+    s.cbr_off[ns] = roff;
+  }
   s.nnz = s.pan_off[ns];
   s.relmap.resize(s.rel_ptr[ns]);
   for (int q = 0; q < ns; ++q) {
