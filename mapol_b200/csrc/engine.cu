@@ -768,9 +768,19 @@ void launch_factor(const LUSystem& sys, int ngroups, const T* A, T* pan, T* cb, 
   const auto it = sys.tuned.find({Prec<T>::idx, ngroups});
   const std::vector<FactorChoice>* tuned = it != sys.tuned.end() ? &it->second : nullptr;
   const size_t n = sys.factor_sched.size();
+  // MPF_FACTOR_KIND=k runs every launch that has a kernel of kind k with that kernel
+  // (the first such candidate), to check that all kinds compute the same factors
+  const char* fk_env = std::getenv("MPF_FACTOR_KIND");
+  const int fk = fk_env ? std::atoi(fk_env) : -1;
   auto one = [&](size_t k, cudaStream_t s) {
     const Launch& ln = sys.factor_sched[k];
-    const FactorChoice ch = tuned ? (*tuned)[k] : heuristic_choice<T>(ln, ngroups);
+    FactorChoice ch = tuned ? (*tuned)[k] : heuristic_choice<T>(ln, ngroups);
+    if (fk >= 0)
+      for (const FactorChoice& c : factor_candidates<T>(ln, ngroups))
+        if (c.kind == fk) {
+          ch = c;
+          break;
+        }
     launch_choice<T>(ch, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, s);
     ++*nlaunch;
   };

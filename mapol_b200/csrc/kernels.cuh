@@ -315,6 +315,7 @@ __global__ void k_check(DevGrid d, int it_arg, int max_it, double tol) {
 // ---------------------------------------------------------------- Newton mismatch
 // grid (row blocks, groups); 8 warps per block; a warp = one bus row x 32 cases.
 constexpr int kRowsPerBlock = 64;
+constexpr int kYB = 2;  // Ybus entries per batch of loads in the mismatch row pass
 
 // With JAC, the same warp then writes the Jacobian entries of its row, reusing the
 // row's admittances, voltages and Ibus; the Jacobian of a case that converges on
@@ -365,16 +366,30 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
     const bool touched = row_touched(o, d.y_diag[i]);
     const double2 vi = d.V[at32(g, d.nb, i, lane)];
     const bool pvi = QL && still_pv(d, i, g, lane);
-    for (int p = p0; p < p1; ++p) {
-      const int j = d.y_col[p];
-      const double2 y = yentry<CTL>(d, o, touched, p, g, lane);
-      const double2 v = j == i ? vi : d.V[at32(g, d.nb, j, lane)];
-      ib.x += y.x * v.x - y.y * v.y;
-      ib.y += y.x * v.y + y.y * v.x;
-      if (JAC && j != i) {
-        const int4 jp = d.jpos[p];
-        if (jp.x >= 0 || jp.y >= 0 || jp.z >= 0 || jp.w >= 0)
-          jac_entry<T>(d, A, g, lane, jp, y, v, vi.x, vi.y, 0.0, 0.0, pvi, QL && still_pv(d, j, g, lane));
+    // kYB entries at a time: their column indices, then their voltages, are loaded
+    // before any of them is used, so the row's chain of dependent loads is one round
+    // trip per kYB entries (padding entries point at the diagonal and load nothing);
+    // Ibus accumulates in the row's order as before
+    for (int p = p0; p < p1; p += kYB) {
+      int jj[kYB];
+      double2 vv[kYB];
+#pragma unroll
+      for (int u = 0; u < kYB; ++u) jj[u] = p + u < p1 ? d.y_col[p + u] : i;
+#pragma unroll
+      for (int u = 0; u < kYB; ++u) vv[u] = jj[u] == i ? vi : d.V[at32(g, d.nb, jj[u], lane)];
+#pragma unroll
+      for (int u = 0; u < kYB; ++u) {
+        if (p + u >= p1) break;
+        const int j = jj[u];
+        const double2 y = yentry<CTL>(d, o, touched, p + u, g, lane);
+        const double2 v = vv[u];
+        ib.x += y.x * v.x - y.y * v.y;
+        ib.y += y.x * v.y + y.y * v.x;
+        if (JAC && j != i) {
+          const int4 jp = d.jpos[p + u];
+          if (jp.x >= 0 || jp.y >= 0 || jp.z >= 0 || jp.w >= 0)
+            jac_entry<T>(d, A, g, lane, jp, y, v, vi.x, vi.y, 0.0, 0.0, pvi, QL && still_pv(d, j, g, lane));
+        }
       }
     }
     double2 s = d.sbus_case ? d.sbus_case[at32(g, d.nb, i, lane)] : d.sbus0[i];
@@ -589,9 +604,12 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
 // reuse a buffer after passing the next pivot's barrier); every thread then
 // updates its own entries from the buffers.  Shared-memory traffic per pivot is
 // 2 TT values per thread for TT^2 multiply-adds, instead of a load and a store
-// of every updated entry.  Same operations per entry, in the same order, as the
-// shared-memory loop of k_mf_factor.  F: the assembled front; on return it holds
-// the factors (and the forward-substituted right-hand side column).
+// of every updated entry.  The pivots run in blocks of 16 (pivot block pt, unrolled):
+// rows and columns of tiles a < pt or b < pt lie above or left of every pivot of the
+// block, so those tiles are final and skipped, and the owner tests are resolved at
+// compile time.  Same operations per live entry, in the same order, as the
+// shared-memory loop of k_mf_factor.  F: the assembled front; on return it holds the
+// factors (and the forward-substituted right-hand side column).
 template <typename T, int V, int TT>
 __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int w, T* cbuf, T* rbuf, int fcap,
                                              int* st_lanes, bool lead) {
@@ -610,78 +628,77 @@ __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int
         for (int k = 0; k < V; ++k) t[a][b].v[k] = (T)0;
       }
     }
-  for (int p = 0; p < w; ++p) {
-    T* cp = cbuf + (p & 1) * fcap * G;        // column p, indexed by row
-    T* rp = rbuf + (p & 1) * (fcap + 1) * G;  // row p, indexed by column
-    const int pr = p & 15, pt = p >> 4;       // owners: thread row / column pr, tile index pt
-    if (c == pr) {
+  int p = 0;
 #pragma unroll
-      for (int a = 0; a < TT; ++a)
+  for (int pt = 0; pt < TT; ++pt) {
+    const int pe = min(w, 16 * (pt + 1));
+    for (; p < pe; ++p) {
+      T* cp = cbuf + (p & 1) * fcap * G;        // column p, indexed by row
+      T* rp = rbuf + (p & 1) * (fcap + 1) * G;  // row p, indexed by column
+      const int pr = p & 15;                    // owners: thread row / column pr
+      if (c == pr) {
 #pragma unroll
-        for (int b = 0; b < TT; ++b) {
+        for (int a = pt; a < TT; ++a) {
           const int i = r + 16 * a;
-          if (b == pt && i >= p && i < f) st<T, V>(cp + i * G, t[a][b]);
+          if (i >= p && i < f) st<T, V>(cp + i * G, t[a][pt]);
         }
-    }
-    if (r == pr) {
+      }
+      if (r == pr) {
 #pragma unroll
-      for (int a = 0; a < TT; ++a)
-#pragma unroll
-        for (int b = 0; b < TT; ++b) {
+        for (int b = pt; b < TT; ++b) {
           const int j = c + 16 * b;
-          if (a == pt && j > p && j < ncols) st<T, V>(rp + j * G, t[a][b]);
+          if (j > p && j < ncols) st<T, V>(rp + j * G, t[pt][b]);
         }
-    }
-    __syncthreads();
-    const LV piv = ld<T, V>(cp + p * G);
-    LV inv;
-#pragma unroll
-    for (int k = 0; k < V; ++k) {
-      T pk = piv.v[k];
-      if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
-        if (lead) mark_singular(&st_lanes[k]);
-        pk = (T)1;
       }
-      inv.v[k] = (T)1 / pk;
-    }
-    // row p's entries right of the pivot and the multipliers of the rows below it;
-    // zero elsewhere, so that the update leaves every other entry as it is (x - 0)
-    LV u[TT], l[TT];
+      __syncthreads();
+      const LV piv = ld<T, V>(cp + p * G);
+      LV inv;
 #pragma unroll
-    for (int b = 0; b < TT; ++b) {
-      const int j = c + 16 * b;
-      if (j > p && j < ncols) u[b] = ld<T, V>(rp + j * G);
-      else {
-#pragma unroll
-        for (int k = 0; k < V; ++k) u[b].v[k] = (T)0;
+      for (int k = 0; k < V; ++k) {
+        T pk = piv.v[k];
+        if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
+          if (lead) mark_singular(&st_lanes[k]);
+          pk = (T)1;
+        }
+        inv.v[k] = (T)1 / pk;
       }
-    }
+      // row p's entries right of the pivot and the multipliers of the rows below it;
+      // zero elsewhere, so that the update leaves every other entry as it is (x - 0)
+      LV u[TT], l[TT];
 #pragma unroll
-    for (int a = 0; a < TT; ++a) {
-      const int i = r + 16 * a;
-      if (i > p && i < f) {
-        l[a] = ld<T, V>(cp + i * G);
+      for (int b = pt; b < TT; ++b) {
+        const int j = c + 16 * b;
+        if (j > p && j < ncols) u[b] = ld<T, V>(rp + j * G);
+        else {
 #pragma unroll
-        for (int k = 0; k < V; ++k) l[a].v[k] *= inv.v[k];
-      } else {
-#pragma unroll
-        for (int k = 0; k < V; ++k) l[a].v[k] = (T)0;
+          for (int k = 0; k < V; ++k) u[b].v[k] = (T)0;
+        }
       }
-    }
 #pragma unroll
-    for (int a = 0; a < TT; ++a)
+      for (int a = pt; a < TT; ++a) {
+        const int i = r + 16 * a;
+        if (i > p && i < f) {
+          l[a] = ld<T, V>(cp + i * G);
 #pragma unroll
-      for (int b = 0; b < TT; ++b)
+          for (int k = 0; k < V; ++k) l[a].v[k] *= inv.v[k];
+        } else {
 #pragma unroll
-        for (int k = 0; k < V; ++k) t[a][b].v[k] = t[a][b].v[k] - l[a].v[k] * u[b].v[k];
-    if (c == pr) {
+          for (int k = 0; k < V; ++k) l[a].v[k] = (T)0;
+        }
+      }
 #pragma unroll
-      for (int a = 0; a < TT; ++a)
+      for (int a = pt; a < TT; ++a)
 #pragma unroll
-        for (int b = 0; b < TT; ++b) {
+        for (int b = pt; b < TT; ++b)
+#pragma unroll
+          for (int k = 0; k < V; ++k) t[a][b].v[k] = t[a][b].v[k] - l[a].v[k] * u[b].v[k];
+      if (c == pr) {
+#pragma unroll
+        for (int a = pt; a < TT; ++a) {
           const int i = r + 16 * a;
-          if (b == pt && i > p && i < f) t[a][b] = l[a];
+          if (i > p && i < f) t[a][pt] = l[a];
         }
+      }
     }
   }
 #pragma unroll
@@ -703,7 +720,7 @@ __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int
 // holds them to at most ~24 warps per SM anyway).  9241-bus workload, mixed solves/s
 // at 64 / 72 / 80 registers: 34.7k / 35.7k / 35.8k (64 spills 48 bytes per thread).
 template <typename T, int G, int TEAM, int TT = 0>
-__global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 1 : (TEAM > 256 ? 1 : (TT < 0 ? 2 : (TEAM == 32 ? 3 : 4)))) k_mf_factor(
+__global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 256 ? 1 : (TT < 0 ? 2 : (TEAM == 32 ? 3 : 4)))) k_mf_factor(
     DevLU L, const int* __restrict__ task_sn, int nsn_l, int ngroups, int fcap,
     const T* __restrict__ A, T* __restrict__ pan, T* __restrict__ cb, T* __restrict__ cbr,
     T* __restrict__ x, int* __restrict__ status, const int* __restrict__ group_active, int with_rhs) {
@@ -1163,6 +1180,9 @@ __global__ void __launch_bounds__(128) k_mf_bsolve(DevLU L, const int* __restric
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     const long long po = L.pan_off[s];
+    // the supernode's U panel (w x f entries of the group) is read pivot row by pivot
+    // row, each row after the last one's solve: one bulk L2 prefetch requests it all
+    if (lane == 0) prefetch_l2(pan + at32(g, L.nnz, po, 0), (unsigned)(w * f) * (32 * sizeof(T)));
     for (int q = 0; q < f; ++q) xs[q * 32 + lane] = x[at32(g, L.n, rows[q], lane)];
     for (int p = w - 1; p >= 0; --p) {
       const T* urow = pan + at32(g, L.nnz, po + (long long)p * f, lane);
@@ -1205,6 +1225,8 @@ __global__ void __launch_bounds__(128) k_mf_bsolve_chunk(DevLU L, const int* __r
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     const long long po = L.pan_off[s];
+    // the U panel of the group, requested from DRAM at once (the chunks of a group share it)
+    if (tid == 0) prefetch_l2(pan + at32(g, L.nnz, po, 0), (unsigned)(w * f) * (32 * sizeof(T)));
     for (int q = slot; q < f; q += SLOTS) xs[q * G + l] = x[at32(g, L.n, rows[q], lane)];
     __syncwarp();
     for (int p = w - 1; p >= 0; --p) {
@@ -1252,6 +1274,7 @@ __global__ void __launch_bounds__(1024) k_mf_bsolve_top(DevLU L, const int* __re
       const int w = L.sn_w[s], f = L.sn_f[s];
       const int* rows = L.sn_rows + L.sn_rptr[s];
       const long long po = L.pan_off[s];
+      if (tid == 0) prefetch_l2(pan + at32(g, L.nnz, po, 0), (unsigned)(w * f) * (32 * sizeof(T)));
       for (int q = slot; q < f; q += SLOTS) xs[q * G + l] = x[at32(g, L.n, rows[q], lane)];
       __syncwarp();
       for (int p = w - 1; p >= 0; --p) {
@@ -1609,6 +1632,9 @@ __global__ void __launch_bounds__(128) k_mf_bsolve_t(DevLU L, const int* __restr
     const int w = L.sn_w[s], f = L.sn_f[s];
     const int* rows = L.sn_rows + L.sn_rptr[s];
     const long long po = L.pan_off[s];
+    // the supernode's panels (U: w x f, L: (f - w) x w entries of the group) are read
+    // column by column, each after the last one's solve: one bulk L2 prefetch for all
+    if (lane == 0) prefetch_l2(pan + at32(g, L.nnz, po, 0), (unsigned)(w * f + (f - w) * w) * (32 * sizeof(T)));
     for (int q = 0; q < f; ++q) xs[q * 32 + lane] = x[at32(g, L.n, rows[q], lane)];
     for (int p = w - 1; p >= 0; --p) {
       T acc = xs[p * 32 + lane];
