@@ -328,10 +328,32 @@ constexpr int kYB = 2;  // Ybus entries per batch of loads in the mismatch row p
 // positions jp (-1: not a J entry).  I = Ibus_i on the diagonal, 0 elsewhere.
 // qrow_off: row i's Q equation is inactive (bus i still PV); vmcol_off: column j's Vm
 // is fixed (bus j still PV).  Inactive entries are 0, the (Q_i, Vm_i) diagonal 1.
-template <typename T>
-__device__ __forceinline__ void jac_entry(const DevGrid& d, T* A, int g, int lane, int4 jp, double2 y, double2 vj,
+// Jacobian entries of one Ybus entry.  The FP32 Jacobian of the mixed form is also
+// computed in FP32 (from the FP64 voltages, admittance and Ibus rounded once): it only
+// feeds the FP32 factorisation, whose rounding it matches, while the mismatch that
+// steers the Newton iteration stays FP64.
+__device__ __forceinline__ void jac_entry(const DevGrid& d, float* A, int g, int lane, int4 jp, double2 y2,
+                                          double2 vj, double a2, double b2, double ir2, double ii2,
+                                          bool qrow_off = false, bool vmcol_off = false, bool diag = false) {
+  const float cc = (float)vj.x, dd = (float)vj.y, yr = (float)y2.x, yi = (float)y2.y;
+  const float a = (float)a2, b = (float)b2, ir = (float)ir2, ii = (float)ii2;
+  const float yvr = yr * cc - yi * dd, yvi = yr * dd + yi * cc;
+  if (jp.x >= 0) A[at32(g, d.nA_jac, jp.x, lane)] = -b * (ir - yvr) - a * (-ii + yvi);
+  if (jp.z >= 0) A[at32(g, d.nA_jac, jp.z, lane)] = qrow_off ? 0.0f : -b * (-ii + yvi) + a * (ir - yvr);
+  if (jp.y >= 0 || jp.w >= 0) {
+    const float inv = rsqrtf(cc * cc + dd * dd);  // 1 / |V_j|
+    const float wr = yvr * inv, wi = yvi * inv;
+    if (jp.y >= 0) A[at32(g, d.nA_jac, jp.y, lane)] = vmcol_off ? 0.0f : a * wr + b * wi + (ir * cc + ii * dd) * inv;
+    if (jp.w >= 0)
+      A[at32(g, d.nA_jac, jp.w, lane)] = (qrow_off || vmcol_off) ? (qrow_off && vmcol_off && diag ? 1.0f : 0.0f)
+                                                                 : -a * wi + b * wr + (ir * dd - ii * cc) * inv;
+  }
+}
+
+__device__ __forceinline__ void jac_entry(const DevGrid& d, double* A, int g, int lane, int4 jp, double2 y, double2 vj,
                                           double a, double b, double ir, double ii, bool qrow_off = false,
                                           bool vmcol_off = false, bool diag = false) {
+  using T = double;
   const double cc = vj.x, dd = vj.y;
   const double yvr = y.x * cc - y.y * dd, yvi = y.x * dd + y.y * cc;
   if (jp.x >= 0) A[at32(g, d.nA_jac, jp.x, lane)] = (T)(-b * (ir - yvr) - a * (-ii + yvi));
@@ -388,7 +410,7 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
         if (JAC && j != i) {
           const int4 jp = d.jpos[p + u];
           if (jp.x >= 0 || jp.y >= 0 || jp.z >= 0 || jp.w >= 0)
-            jac_entry<T>(d, A, g, lane, jp, y, v, vi.x, vi.y, 0.0, 0.0, pvi, QL && still_pv(d, j, g, lane));
+            jac_entry(d, A, g, lane, jp, y, v, vi.x, vi.y, 0.0, 0.0, pvi, QL && still_pv(d, j, g, lane));
         }
       }
     }
@@ -412,7 +434,7 @@ __global__ void __launch_bounds__(256, 4) k_mismatch_nr(DevGrid d, T* x, T* A) {
     if (JAC) {
       const int pd = d.y_diag[i];
       const int4 jp = d.jpos[pd];
-      jac_entry<T>(d, A, g, lane, jp, yentry<CTL>(d, o, touched, pd, g, lane), vi, vi.x, vi.y, ib.x, ib.y, pvi, pvi,
+      jac_entry(d, A, g, lane, jp, yentry<CTL>(d, o, touched, pd, g, lane), vi, vi.x, vi.y, ib.x, ib.y, pvi, pvi,
                    true);
     } else {
       d.Ibus[at32(g, d.nb, i, lane)] = ib;
@@ -561,6 +583,21 @@ __global__ void k_fd_outage(DevGrid d, int nA, const int4* br_apos, const double
 //      J is factorised in the same static order for every case);
 //   4. store the U- and L-panels, the forward-substituted y of the pivots, and
 //      the contribution block for the parent.
+// A pivot that is zero, subnormal or the smallest normal value, infinite or NaN, tested
+// in the pivot's own precision
+__device__ __forceinline__ bool bad_pivot(float pk) { return !(fabsf(pk) > FLT_MIN) || !(fabsf(pk) <= FLT_MAX); }
+__device__ __forceinline__ bool bad_pivot(double pk) { return !(fabs(pk) > DBL_MIN) || !(fabs(pk) <= DBL_MAX); }
+
+// Advances task (q, r) by a stride of sq whole supernodes and sr lane chunks (r < nch)
+__device__ __forceinline__ void next_task(int& q, int& r, int sq, int sr, int nch) {
+  q += sq;
+  r += sr;
+  if (r >= nch) {
+    r -= nch;
+    ++q;
+  }
+}
+
 template <int TEAM>
 __device__ __forceinline__ void team_sync() {
   if (TEAM == 32) __syncwarp();
@@ -656,7 +693,7 @@ __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int
 #pragma unroll
       for (int k = 0; k < V; ++k) {
         T pk = piv.v[k];
-        if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
+        if (bad_pivot(pk)) {
           if (lead) mark_singular(&st_lanes[k]);
           pk = (T)1;
         }
@@ -742,11 +779,16 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
   const int slot = tid / NV, lv = (tid % NV) * V;
   const int rs = slot % RSL, cg = slot / RSL;
   T* F = reinterpret_cast<T*>(smem_raw) + (size_t)team * fcap * front_stride(fcap) * G + lv;
-  const long long nchunks = (long long)ngroups * LPG;
-  const long long ntasks = (long long)nsn_l * nchunks;
-  for (long long t = (long long)blockIdx.x * teams + team; t < ntasks; t += (long long)gridDim.x * teams) {
-    const int s = task_sn[t / nchunks];
-    const int ch = (int)(t % nchunks);
+  // Task t = q * nch + r is lane chunk r of the launch's q-th supernode.  Teams stride
+  // over t by gridDim.x * teams (< 2^31, as are nch and q); q and r advance by the
+  // stride's quotient and remainder, so no task needs a 64-bit division.
+  const int nch = ngroups * LPG;
+  const int tstride = gridDim.x * teams;
+  const int sq = tstride / nch, sr = tstride % nch;
+  for (int q = (blockIdx.x * teams + team) / nch, r = (blockIdx.x * teams + team) % nch; q < nsn_l;
+       next_task(q, r, sq, sr, nch)) {
+    const int s = task_sn[q];
+    const int ch = r;
     const int g = ch / LPG;
     if (!group_active[g] || !task_here(L, s, g)) continue;
     const int lane = (ch % LPG) * G + lv;  // first of this thread's V lanes
@@ -774,6 +816,17 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
       if (tid == 1 && cin.ncb > 0) prefetch_l2(cb + at32(g, L.sumcb, cin.cb, 0), (unsigned)cin.ncb * B32);
       if (tid == 2 && with_rhs && cin.ncbr > 0) prefetch_l2(cbr + at32(g, L.sumcbr, cin.cbr, 0), (unsigned)cin.ncbr * B32);
     }
+    // the first child's reference and this thread's first arrowhead positions, loaded
+    // before the front is zeroed so that their latency overlaps the zeroing (larger
+    // teams: more slots per front and fewer registers, so fewer positions per thread)
+    ChildRef next = ci0 < ci1 ? L.child_ref[ci0] : ChildRef{};
+    constexpr int H = TEAM == 32 ? (sizeof(T) == 4 ? 8 : 4) : (TT > 0 ? 1 : 2);
+    int loc0[H];
+#pragma unroll
+    for (int u = 0; u < H; ++u) {
+      const int e = ah0 + slot + u * SLOTS;
+      loc0[u] = e < ah1 ? L.ah_loc[e] : 0;
+    }
     // F + (r * RS + c) * G: entry (r, c) of this thread's lanes
 #define FP(r, c) (F + ((r) * RS + (c)) * G)
     {
@@ -790,6 +843,10 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
       const T* a0 = A + at32(g, L.nA, 0, lane);
       const int e1 = ah1;
       int e = ah0 + slot;
+#pragma unroll
+      for (int u = 0; u < H; ++u)
+        if (e + u * SLOTS < e1) cp_async<T, V>(F + loc0[u] * G, a0 + (size_t)(e + u * SLOTS) * 32);
+      e += H * SLOTS;
       for (; e + 7 * SLOTS < e1; e += 8 * SLOTS) {
         int loc[8];
 #pragma unroll
@@ -803,7 +860,6 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
       asm volatile("cp.async.wait_all;\n" ::: "memory");
     }
     team_sync<TEAM>();
-    ChildRef next = ci0 < ci1 ? L.child_ref[ci0] : ChildRef{};
     for (int ci = ci0; ci < ci1; ++ci) {
       // the next child's reference is loaded while this one is added
       const ChildRef cr = next;
@@ -874,7 +930,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
 #pragma unroll
       for (int k = 0; k < V; ++k) {
         T pk = piv.v[k];
-        if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
+        if (bad_pivot(pk)) {
           if (slot == 0) mark_singular(&status[g * 32 + lane + k]);
           pk = (T)1;
         }
@@ -1024,7 +1080,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
 #pragma unroll
       for (int k = 0; k < V; ++k) {
         T pk = piv.v[k];
-        if (!(fabs((double)pk) > (sizeof(T) == 8 ? DBL_MIN : FLT_MIN)) || !(fabs((double)pk) <= DBL_MAX)) {
+        if (bad_pivot(pk)) {
           if (slot == 0) mark_singular(&status[g * 32 + lane + k]);
           pk = (T)1;
         }

@@ -64,15 +64,18 @@ def test_config2_full_size_matches_oracle(gpu):
 
 def test_one_batch_launches_like_its_largest_grid(cfg2):
     """The stages of all grids share launches: a three-grid solve launches about as
-    many kernels as its largest grid alone, not the sum of the three."""
+    many kernels as its largest grid alone, not the sum of the three.  The fixed
+    kernel rule is used (no autotuning): the tuner may fold the backward solve's
+    near-root levels into one launch for one batch and not for another, which changes
+    launch counts without changing what this test is about."""
     grids, cases = cfg2
     launches = []
     for (b, br), cs in zip(grids, cases):
-        with m.PowerFlow(b, br) as pf:
+        with m.PowerFlow(b, br, autotune=0) as pf:
             pf.set_cases(cs)
             pf.solve(m.NR, m.MIXED)
             launches.append(pf.timing()["launches"])
-    with m.MultiGrid(grids) as mg:
+    with m.MultiGrid(grids, autotune=0) as mg:
         mg.set_cases(cases)
         mg.solve(m.NR, m.MIXED)
         joint = mg.timing()["launches"]
