@@ -617,6 +617,29 @@ template <typename T, int V>
 __device__ __forceinline__ Lanes<T, V> ld(const T* p) { return *reinterpret_cast<const Lanes<T, V>*>(p); }
 template <typename T, int V>
 __device__ __forceinline__ void st(T* p, const Lanes<T, V>& a) { *reinterpret_cast<Lanes<T, V>*>(p) = a; }
+// Pivot inverses, one division per thread: every thread of a warp inverts the pivot of
+// lane ml = (warp lane) % G of its task's G lanes (own_inverse; a bad pivot is replaced
+// by 1 and marks its case SINGULAR, by the marker threads, one per lane), and the V
+// inverses a thread carries (lanes lv .. lv + V - 1) reach it by shuffles from threads
+// lv .. lv + V - 1, which inverted exactly those lanes (gather_lanes; all 32 threads of
+// the warp call it together).  A warp thus runs one IEEE division per thread instead
+// of V, with the same quotients.
+template <typename T, int G>
+__device__ __forceinline__ T own_inverse(T pk, bool marker, int* st_lane0) {
+  if (bad_pivot(pk)) {
+    if (marker) mark_singular(&st_lane0[(threadIdx.x & 31) % G]);
+    pk = (T)1;
+  }
+  return (T)1 / pk;
+}
+template <typename T, int V>
+__device__ __forceinline__ Lanes<T, V> gather_lanes(T own, int lv) {
+  Lanes<T, V> r;
+#pragma unroll
+  for (int k = 0; k < V; ++k) r.v[k] = __shfl_sync(0xffffffffu, own, lv + k);
+  return r;
+}
+
 // V adjacent lanes of one entry copied global -> shared asynchronously (cp.async, cache
 // at all levels); both addresses aligned to the copy size; completes at the next
 // cp.async.wait_all of the issuing thread
@@ -688,17 +711,8 @@ __device__ __forceinline__ void lu_registers(T* F, int RS, int f, int ncols, int
         }
       }
       __syncthreads();
-      const LV piv = ld<T, V>(cp + p * G);
-      LV inv;
-#pragma unroll
-      for (int k = 0; k < V; ++k) {
-        T pk = piv.v[k];
-        if (bad_pivot(pk)) {
-          if (lead) mark_singular(&st_lanes[k]);
-          pk = (T)1;
-        }
-        inv.v[k] = (T)1 / pk;
-      }
+      // one thread per entry carries all G = V lanes (lv = 0)
+      const LV inv = gather_lanes<T, V>(own_inverse<T, G>(cp[p * G + (threadIdx.x & 31) % G], threadIdx.x < G, st_lanes), 0);
       // row p's entries right of the pivot and the multipliers of the rows below it;
       // zero elsewhere, so that the update leaves every other entry as it is (x - 0)
       LV u[TT], l[TT];
@@ -925,19 +939,12 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
     // start of the next step (no thread reads them there) or after the last one.
     // Every entry sees the operations of the one-pivot loop in the same order, so the
     // factors are the same bit for bit.
-    auto pivot_inverse = [&](LV piv) {
-      LV inv;
-#pragma unroll
-      for (int k = 0; k < V; ++k) {
-        T pk = piv.v[k];
-        if (bad_pivot(pk)) {
-          if (slot == 0) mark_singular(&status[g * 32 + lane + k]);
-          pk = (T)1;
-        }
-        inv.v[k] = (T)1 / pk;
-      }
-      return inv;
-    };
+    // lane ml of the task's chunk (the lane whose pivots this thread inverts) and the
+    // threads that mark a bad pivot's case
+    const T* Fl = F - lv;
+    const int ml = (threadIdx.x & 31) % G;
+    const bool marker = tid < G;
+    int* st0 = status + g * 32 + (lane - lv);
     int pend = 0, pc = 0;  // deferred work of the last step: 1 = one pivot pc, 2 = pivots pc, pc + 1
     LV pinv0, pinv1, pu, pl;
     auto finish = [&]() {
@@ -976,17 +983,18 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
       pend = 0;
     };
     for (int p = 0; p < w;) {
-      const LV inv0 = pivot_inverse(ld<T, V>(FP(p, p)));
+      const T i0 = own_inverse<T, G>(Fl[(p * RS + p) * G + ml], marker, st0);
+      const LV inv0 = gather_lanes<T, V>(i0, lv);
       if (p + 1 < w) {
         const int p1 = p + 1;
         const LV u = ld<T, V>(FP(p, p1));
-        LV l = ld<T, V>(FP(p1, p)), piv1 = ld<T, V>(FP(p1, p1));
+        LV l = ld<T, V>(FP(p1, p));
 #pragma unroll
-        for (int k = 0; k < V; ++k) {
-          l.v[k] *= inv0.v[k];
-          piv1.v[k] = piv1.v[k] - l.v[k] * u.v[k];
-        }
-        const LV inv1 = pivot_inverse(piv1);
+        for (int k = 0; k < V; ++k) l.v[k] *= inv0.v[k];
+        // the second pivot of lane ml, updated by the first one: F(p1,p1) - l u
+        const T lm = Fl[(p1 * RS + p) * G + ml] * i0;
+        const T pk1 = Fl[(p1 * RS + p1) * G + ml] - lm * Fl[(p * RS + p1) * G + ml];
+        const LV inv1 = gather_lanes<T, V>(own_inverse<T, G>(pk1, marker, st0), lv);
         finish();
         const int nq = ncols - (p1 + 1);
         const int q0 = p1 + 1 + (nq * cg) / CG, q1 = p1 + 1 + (nq * (cg + 1)) / CG;
@@ -1075,17 +1083,9 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
     // column p any more (and after the loop for the last pivot).
     LV inv_prev;
     for (int p = 0; p < w; ++p) {
-      const LV piv = ld<T, V>(FP(p, p));
-      LV inv;
-#pragma unroll
-      for (int k = 0; k < V; ++k) {
-        T pk = piv.v[k];
-        if (bad_pivot(pk)) {
-          if (slot == 0) mark_singular(&status[g * 32 + lane + k]);
-          pk = (T)1;
-        }
-        inv.v[k] = (T)1 / pk;
-      }
+      const LV inv = gather_lanes<T, V>(
+          own_inverse<T, G>(F[(p * RS + p) * G - lv + (threadIdx.x & 31) % G], tid < G, status + g * 32 + (lane - lv)),
+          lv);
       if (p > 0 && cg == CG - 1)
         for (int i = p + rs; i < f; i += RSL) {
           LV c = ld<T, V>(FP(i, p - 1));
