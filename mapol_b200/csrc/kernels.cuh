@@ -1078,15 +1078,16 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
     team_sync<TEAM>();
     } else {
     // Right-looking partial LU of the w pivots, one team barrier per pivot.  At
-    // pivot p every thread reads the unscaled column p (l_ip = F(i,p) / F(p,p));
-    // the scaled values are written back one pivot later, when no thread reads
-    // column p any more (and after the loop for the last pivot).
+    // pivot p the threads of row i read the unscaled F(i,p) (l_ip = F(i,p) / F(p,p)).
+    // With one column group (CG = 1: each row has one owner slot) the owner writes l_ip
+    // back at once; otherwise the scaled values are written back one pivot later, when
+    // no thread reads column p any more (and after the loop for the last pivot).
     LV inv_prev;
     for (int p = 0; p < w; ++p) {
       const LV inv = gather_lanes<T, V>(
           own_inverse<T, G>(F[(p * RS + p) * G - lv + (threadIdx.x & 31) % G], tid < G, status + g * 32 + (lane - lv)),
           lv);
-      if (p > 0 && cg == CG - 1)
+      if (CG > 1 && p > 0 && cg == CG - 1)
         for (int i = p + rs; i < f; i += RSL) {
           LV c = ld<T, V>(FP(i, p - 1));
 #pragma unroll
@@ -1101,6 +1102,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
         LV lip = ld<T, V>(ri + p * G);
 #pragma unroll
         for (int k = 0; k < V; ++k) lip.v[k] *= inv.v[k];
+        if constexpr (CG == 1) st<T, V>(ri + p * G, lip);
         int q = q0;
         for (; q + U <= q1; q += U) {
           LV a[U], b[U];
@@ -1127,7 +1129,7 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
       inv_prev = inv;
       team_sync<TEAM>();
     }
-    if (w > 0) {
+    if (CG > 1 && w > 0) {
       if (cg == CG - 1)
         for (int i = w + rs; i < f; i += RSL) {
           LV c = ld<T, V>(FP(i, w - 1));
