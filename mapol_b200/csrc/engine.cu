@@ -81,7 +81,7 @@ void upload(DevBuf& b, const std::vector<T>& v) {
 }
 
 // ------------------------------------------------------------------ LU system
-enum TaskClass { CLS_S = 0, CLS_M = 1, CLS_L = 2, CLS_M1 = 3 };
+enum TaskClass { CLS_S = 0, CLS_M = 1, CLS_L = 2, CLS_M1 = 3, CLS_BIG = 4 };
 // fronts up to kFmaxS: one case per thread; up to kFmaxM: a warp per 32-byte lane
 // chunk; larger: a 256-thread block per lane chunk, with fewer lanes per task when a
 // 32-byte chunk would not fit in shared memory (kSmemMax)
@@ -89,8 +89,33 @@ constexpr int kFmaxS = 8, kFmaxM1 = 16, kFmaxM = 24;
 constexpr size_t kSmemMax = 227 * 1024;
 // rounds of PV -> PQ switching per solve (each switches at least one bus of a case)
 constexpr int kMaxQRounds = 20;
-// largest front any task class can hold: one FP64 lane, f * ((f + 1) | 1) * 8 bytes
+// largest dense front in shared memory: one FP64 lane, f * ((f + 1) | 1) * 8 bytes.
+// Larger fronts (CLS_BIG, densely meshed grids) keep only their panel, w (2f - w + 1)
+// entries, in shared memory (k_mf_factor_big) and their trailing block in global memory
 constexpr int kFmaxAll = 167;
+inline size_t big_panel(int w, int f) { return (size_t)w * (2 * f - w + 1); }
+// The fronts' limits: every panel of one FP64 lane and one warp's slice of x in the
+// thread-per-case substitutions (f entries of 32 FP64 lanes) fit in shared memory
+inline std::string front_limits(const LUSymbolic& L, const char* what) {
+  for (int s = 0; s < L.nsn; ++s) {
+    const int w = L.sn_w[s], f = L.sn_f[s];
+    if (f > kFmaxAll && big_panel(w, f) * 8 > kSmemMax)
+      return std::string(what) + ": a front of " + std::to_string(f) + " rows with " + std::to_string(w) +
+             " pivots needs a " + std::to_string(big_panel(w, f) * 8 / 1024) + " KB panel, above the " +
+             std::to_string(kSmemMax / 1024) + " KB of shared memory (grid too densely meshed)";
+    if ((size_t)f * 32 * 8 > kSmemMax)
+      return std::string(what) + ": a front of " + std::to_string(f) + " rows exceeds " +
+             std::to_string(kSmemMax / 256) + " (grid too densely meshed)";
+  }
+  return {};
+}
+// warps per block of the substitution kernels that hold a warp's slice of x (fcap
+// entries of `lanes` lanes) in shared memory: four, or fewer for large fronts
+template <typename T>
+int solve_warps(int fcap, int lanes) {
+  const size_t per = (size_t)std::max(fcap, 1) * lanes * sizeof(T);
+  return (int)std::max<size_t>(1, std::min<size_t>(4, kSmemMax / per));
+}
 // backward solve: levels nearest the root with at most this many supernodes can run as
 // one k_mf_bsolve_top launch (an autotuner choice); codes kTopCode + G in the tuned
 // per-launch choices mark the launches it replaces
@@ -107,6 +132,7 @@ struct Launch {
   int offset, count, cls, fcap;  // range of lev_sn, task class, max front in range
   int wfmax = 0;                 // largest w * f in range (U-panel entries)
   int level = 0;                 // elimination-tree level
+  size_t pcap = 0;               // CLS_BIG: largest panel in range, w (2f - w + 1) entries
 };
 
 // Side streams of one LU system, created on first use.  The factorisation's launches
@@ -305,7 +331,7 @@ struct LUSystem {
       int k = b;
       while (k < e) {
         auto cls_of = [](int f) {
-          return f <= kFmaxS ? CLS_S : f <= kFmaxM1 ? CLS_M1 : f <= kFmaxM ? CLS_M : CLS_L;
+          return f <= kFmaxS ? CLS_S : f <= kFmaxM1 ? CLS_M1 : f <= kFmaxM ? CLS_M : f <= kFmaxAll ? CLS_L : CLS_BIG;
         };
         const int cls = cls_of(s.sn_f[s.lev_sn[k]]);
         int k2 = k, fcap = 0;
@@ -323,6 +349,10 @@ struct LUSystem {
     // the backward substitution's launches and their DAG (top-down: parents first)
     bsolve_sched = factor_sched;
     split_factor_launches(s);
+    for (Launch& ln : factor_sched)
+      if (ln.cls == CLS_BIG)
+        for (int t = ln.offset; t < ln.offset + ln.count; ++t)
+          ln.pcap = std::max(ln.pcap, big_panel(s.sn_w[s.lev_sn[t]], s.sn_f[s.lev_sn[t]]));
     for (const Launch& ln : factor_sched) {
       fingerprint = (fingerprint ^ (uint64_t)ln.offset) * 1099511628211ull;
       fingerprint = (fingerprint ^ (uint64_t)ln.count) * 1099511628211ull;
@@ -541,6 +571,11 @@ void ensure_attrs(int device) {
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_chunk<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_fsolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_fsolve_t<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_t<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
@@ -567,6 +602,26 @@ void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const
   k_mf_factor<T, G, TEAM, TT><<<(unsigned)blocks, TEAM * teams_per_block, smem, st>>>(
       sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups, ln.fcap, A, pan, cb, cbr, x, status,
       group_active, with_rhs);
+  CUDA_TRY(cudaGetLastError());
+}
+
+// Fronts too large for a dense front in shared memory: k_mf_factor_big, a 256-thread
+// block per (supernode, chunk of ge lanes), the launch's largest panel in shared memory
+template <typename T>
+void launch_factor_big(int ge, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr,
+                       T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
+  const size_t smem = ln.pcap * ge * sizeof(T);
+  if (ln.pcap == 0 || smem > kSmemMax) throw MpfError{MPF_ERR_INTERNAL, "big-front panel does not fit"};
+  const long long ntasks = (long long)ln.count * ngroups * (32 / ge);
+  const unsigned blocks = (unsigned)std::min<long long>(ntasks, 148LL * 32);
+  const DevLU dl = sys.dev();
+  const int* ts = sys.lev_sn.as<int>() + ln.offset;
+  switch (ge) {
+    case 4: k_mf_factor_big<T, 4><<<blocks, 256, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    case 2: k_mf_factor_big<T, 2><<<blocks, 256, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    case 1: k_mf_factor_big<T, 1><<<blocks, 256, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    default: throw MpfError{MPF_ERR_INTERNAL, "no big-front kernel for this lane count"};
+  }
   CUDA_TRY(cudaGetLastError());
 }
 
@@ -649,6 +704,12 @@ template <typename T>
 FactorChoice heuristic_choice(const Launch& ln, int ngroups) {
   constexpr int G = Prec<T>::G;
   const long long lanes_tasks = (long long)ln.count * ngroups;
+  if (ln.cls == CLS_BIG) {
+    // panels in shared memory: as many lanes per task as the largest panel allows
+    int ge = std::min(G, 4);
+    while (ge > 1 && ln.pcap * ge * sizeof(T) > kSmemMax) ge /= 2;
+    return {6, ge, 0, 1};
+  }
   if (ln.cls == CLS_S && lanes_tasks < kMinWarpTasks) return {1, 32, 0, 1};
   if ((ln.cls == CLS_M1 || ln.cls == CLS_M) && lanes_tasks * (32 / G) < kMinWarpTasks) {
     int ge = G;
@@ -672,6 +733,7 @@ std::vector<FactorChoice> factor_candidates(const Launch& ln, int ngroups) {
   constexpr int G = Prec<T>::G;
   const size_t ws = sizeof(T);
   std::vector<FactorChoice> c{heuristic_choice<T>(ln, ngroups)};
+  if (ln.cls == CLS_BIG) return c;  // one kernel holds fronts of this size
   auto add = [&](FactorChoice x) {
     for (const auto& y : c)
       if (y.kind == x.kind && y.ge == x.ge && y.tt == x.tt && y.tpb == x.tpb) return;
@@ -733,6 +795,8 @@ void launch_choice(const FactorChoice& ch, const LUSystem& sys, const Launch& ln
       launch_factor_ge<T>(ch.ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
   } else if (ch.kind == 2) {
     launch_factor_reg<T>(ch.ge, ch.tt, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+  } else if (ch.kind == 6) {
+    launch_factor_big<T>(ch.ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
   } else if (ch.kind == 5) {
     const bool wide = ch.tpb == 2;
     if (ch.ge == G && wide)
@@ -992,15 +1056,17 @@ void launch_bsolve_one(int ge, const LUSystem& sys, const Launch& ln, int ngroup
     return;
   }
   const long long ntasks = (long long)ln.count * ngroups * (ge ? 32 / ge : 1);
-  const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-  const size_t smem = (size_t)4 * ln.fcap * (ge ? ge : 32) * sizeof(T);
+  const int wpb = solve_warps<T>(ln.fcap, ge ? ge : 32);
+  const long long blocks = std::min<long long>((ntasks + wpb - 1) / wpb, 148LL * 32);
+  const size_t smem = (size_t)wpb * ln.fcap * (ge ? ge : 32) * sizeof(T);
+  const unsigned nt = 32 * wpb;
   switch (ge) {
-    case 0: k_mf_bsolve<T><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-    case 16: k_mf_bsolve_chunk<T, 16><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-    case 8: k_mf_bsolve_chunk<T, 8><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-    case 4: k_mf_bsolve_chunk<T, 4><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-    case 2: k_mf_bsolve_chunk<T, 2><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
-    case 1: k_mf_bsolve_chunk<T, 1><<<(unsigned)blocks, 128, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 0: k_mf_bsolve<T><<<(unsigned)blocks, nt, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 16: k_mf_bsolve_chunk<T, 16><<<(unsigned)blocks, nt, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 8: k_mf_bsolve_chunk<T, 8><<<(unsigned)blocks, nt, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 4: k_mf_bsolve_chunk<T, 4><<<(unsigned)blocks, nt, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 2: k_mf_bsolve_chunk<T, 2><<<(unsigned)blocks, nt, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
+    case 1: k_mf_bsolve_chunk<T, 1><<<(unsigned)blocks, nt, smem, st>>>(dl, ts, ln.count, ngroups, ln.fcap, pan, x, group_active); break;
     default: throw MpfError{MPF_ERR_INTERNAL, "no backward-solve kernel for this lane count"};
   }
   CUDA_TRY(cudaGetLastError());
@@ -1242,9 +1308,10 @@ void launch_fsolve(const LUSystem& sys, int ngroups, const T* pan, T* cbr, T* x,
                    cudaStream_t st, int* nlaunch) {
   for (const Launch& ln : sys.level_sched) {
     const long long ntasks = (long long)ln.count * ngroups;
-    long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-    const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
-    k_mf_fsolve<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups,
+    const int wpb = solve_warps<T>(ln.fcap, 32);
+    long long blocks = std::min<long long>((ntasks + wpb - 1) / wpb, 148LL * 32);
+    const size_t smem = (size_t)wpb * ln.fcap * 32 * sizeof(T);
+    k_mf_fsolve<T><<<(unsigned)blocks, 32 * wpb, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count, ngroups,
                                                         ln.fcap, pan, cbr, x, group_active);
     CUDA_TRY(cudaGetLastError());
     ++*nlaunch;
@@ -1902,9 +1969,10 @@ void launch_fsolve_t(const LUSystem& sys, int ngroups, const T* pan, T* cbr, T* 
                      cudaStream_t st) {
   for (const Launch& ln : sys.level_sched) {
     const long long ntasks = (long long)ln.count * ngroups;
-    const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-    const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
-    k_mf_fsolve_t<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
+    const int wpb = solve_warps<T>(ln.fcap, 32);
+    const long long blocks = std::min<long long>((ntasks + wpb - 1) / wpb, 148LL * 32);
+    const size_t smem = (size_t)wpb * ln.fcap * 32 * sizeof(T);
+    k_mf_fsolve_t<T><<<(unsigned)blocks, 32 * wpb, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
                                                           ngroups, ln.fcap, pan, cbr, x, group_active);
     CUDA_TRY(cudaGetLastError());
   }
@@ -1915,9 +1983,10 @@ void launch_bsolve_t(const LUSystem& sys, int ngroups, const T* pan, T* x, const
   for (int k = (int)sys.level_sched.size() - 1; k >= 0; --k) {
     const Launch& ln = sys.level_sched[k];
     const long long ntasks = (long long)ln.count * ngroups;
-    const long long blocks = std::min<long long>((ntasks + 3) / 4, 148LL * 32);
-    const size_t smem = (size_t)4 * ln.fcap * 32 * sizeof(T);
-    k_mf_bsolve_t<T><<<(unsigned)blocks, 128, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
+    const int wpb = solve_warps<T>(ln.fcap, 32);
+    const long long blocks = std::min<long long>((ntasks + wpb - 1) / wpb, 148LL * 32);
+    const size_t smem = (size_t)wpb * ln.fcap * 32 * sizeof(T);
+    k_mf_bsolve_t<T><<<(unsigned)blocks, 32 * wpb, smem, st>>>(sys.dev(), sys.lev_sn.as<int>() + ln.offset, ln.count,
                                                           ngroups, ln.fcap, pan, x, group_active);
     CUDA_TRY(cudaGetLastError());
   }
@@ -2068,12 +2137,14 @@ int32_t mpf_create(const mpf_bus* buses, int32_t n_bus, const mpf_branch* branch
     if (find_bridges(branches, n_branch, n_bus, h->is_bridge) != 0)
       return fail(h.get(), MPF_ERR_BAD_INPUT, "bridge search failed");
     const GridSymbolic& g = h->g;
-    int maxf = g.jac.max_front;
-    for (int v = 0; v < 2; ++v) maxf = std::max({maxf, g.bp[v].lu.max_front, g.bpp[v].lu.max_front});
-    if (maxf > kFmaxAll)
-      return fail(h.get(), MPF_ERR_BAD_INPUT,
-                  "largest frontal matrix (" + std::to_string(maxf) + ") exceeds the supported " +
-                      std::to_string(kFmaxAll) + " (grid too densely meshed for shared-memory fronts)");
+    {
+      std::string lim = front_limits(g.jac, "Newton system");
+      for (int v = 0; v < 2 && lim.empty(); ++v) {
+        lim = front_limits(g.bp[v].lu, "B'");
+        if (lim.empty()) lim = front_limits(g.bpp[v].lu, "B''");
+      }
+      if (!lim.empty()) return fail(h.get(), MPF_ERR_BAD_INPUT, lim);
+    }
     CUDA_TRY(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaMallocHost(&h->h_any, sizeof(int)));
     CUDA_TRY(cudaEventCreate(&h->t0));
@@ -2560,9 +2631,10 @@ int32_t mpf_set_q_limits(mpf_handle* h, const double* qmin, const double* qmax) 
     const std::string msg = build_symbolic(h->buses.data(), nb, h->branches.data(), (int)h->branches.size(), g2,
                                            swb.empty() ? nullptr : &vf, h->opt.ordering);
     if (!msg.empty()) return fail(h, MPF_ERR_BAD_INPUT, msg);
-    if (g2.jac.max_front > kFmaxAll)
-      return fail(h, MPF_ERR_BAD_INPUT, "largest frontal matrix with the limited PV buses exceeds " +
-                                            std::to_string(kFmaxAll));
+    {
+      const std::string lim = front_limits(g2.jac, "Newton system with the limited PV buses");
+      if (!lim.empty()) return fail(h, MPF_ERR_BAD_INPUT, lim);
+    }
     for (int p = 0; p < 2; ++p) h->nr_graph[p].release();
     h->jac.release_values();
     h->jac.tuned.clear();

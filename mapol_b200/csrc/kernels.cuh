@@ -1179,6 +1179,148 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
   }
 }
 
+// Fronts too large for a dense front in shared memory (densely meshed grids).  Only
+// the panel lives in shared memory: the w pivot rows with all f columns and the
+// right-hand side (top part, w x (f + 1)) and the pivot columns of the other rows (left
+// part, m x w, m = f - w), G lanes per entry.  The trailing m x m block is the
+// supernode's contribution block itself, in global memory: zeroed, the children's
+// entries added into it where they fall, and the Schur complement applied there after
+// the panel's LU.  Every entry takes the same operations in the same order as in the
+// one-pivot loop of k_mf_factor (assignment of the arrowhead value, the children's
+// additions in child order, then x - l_ip u_pj for p = 0 .. w - 1), so the factors are
+// the same bit for bit.  One 256-thread block per task (supernode, chunk of G lanes);
+// thread = (entry slot, lane); dynamic shared memory: the launch's largest panel.
+template <typename T, int G>
+__global__ void __launch_bounds__(256) k_mf_factor_big(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+                                                       int ngroups, const T* __restrict__ A,
+                                                       T* __restrict__ pan, T* __restrict__ cb,
+                                                       T* __restrict__ cbr, T* __restrict__ x,
+                                                       int* __restrict__ status,
+                                                       const int* __restrict__ group_active, int with_rhs) {
+  constexpr int SLOTS = 256 / G, LPG = 32 / G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* P = reinterpret_cast<T*>(smem_raw);
+  const int slot = threadIdx.x / G, l = threadIdx.x % G;
+  const int nch = ngroups * LPG;
+  for (int q = blockIdx.x / nch, ch = blockIdx.x % nch; q < nsn_l;
+       next_task(q, ch, (int)gridDim.x / nch, (int)gridDim.x % nch, nch)) {
+    const int s = task_sn[q];
+    const int g = ch / LPG;
+    if (!group_active[g] || !task_here(L, s, g)) continue;  // uniform over the block
+    const int lane = (ch % LPG) * G + l;
+    const int w = L.sn_w[s], f = L.sn_f[s], m = f - w;
+    const int* rows = L.sn_rows + L.sn_rptr[s];
+    const int RS = front_stride(f);
+    const int ncols = with_rhs ? f + 1 : f;
+    const bool has_parent = L.sn_parent[s] >= 0;
+    const long long cbo = L.cb_off[s], cbro = L.cbr_off[s];
+    const int npan = w * (f + 1) + m * w;
+    // panel entry (r, c), r < w or c < w: top part row-major, then the left part
+    auto PE = [&](int r, int c) -> T& {
+      return r < w ? P[((size_t)r * (f + 1) + c) * G + l] : P[((size_t)w * (f + 1) + (size_t)(r - w) * w + c) * G + l];
+    };
+    // trailing entry (a, b) of the contribution block, and the carried right-hand side
+    auto CE = [&](int a, int b) -> T& { return cb[at32(g, L.sumcb, cbo + (long long)a * m + b, lane)]; };
+    auto CR = [&](int a) -> T& { return cbr[at32(g, L.sumcbr, cbro + a, lane)]; };
+    const bool trail = has_parent && m > 0;
+    for (int e = slot; e < npan; e += SLOTS) P[(size_t)e * G + l] = (T)0;
+    if (trail) {
+      for (int e = slot; e < m * m; e += SLOTS) CE(e / m, e % m) = (T)0;
+      if (with_rhs)
+        for (int a = slot; a < m; a += SLOTS) CR(a) = (T)0;
+    }
+    __syncthreads();
+    // the arrowhead: pivot rows and pivot columns, all in the panel
+    {
+      const int e0 = L.ah_ptr[s], e1 = L.ah_ptr[s + 1];
+      for (int e = e0 + slot; e < e1; e += SLOTS) {
+        const int loc = L.ah_loc[e];
+        PE(loc / RS, loc % RS) = A[at32(g, L.nA, e, lane)];
+      }
+      if (with_rhs)
+        for (int p = slot; p < w; p += SLOTS) PE(p, f) = x[at32(g, L.n, rows[p], lane)];
+    }
+    __syncthreads();
+    // the children's contribution blocks, one child after the other (siblings may add
+    // into the same entries; within a child the relative map is injective)
+    for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
+      const ChildRef cr = L.child_ref[ci];
+      const int mc = cr.m;
+      const int* rel = L.relmap + cr.rel_ptr;
+      for (int e = slot; e < mc * mc; e += SLOTS) {
+        const int r = rel[e / mc], c = rel[e % mc];
+        const T v = cb[at32(g, L.sumcb, cr.cb_off + e, lane)];
+        if (r < w || c < w) PE(r, c) += v;
+        else if (trail) CE(r - w, c - w) += v;
+      }
+      if (with_rhs)
+        for (int a = slot; a < mc; a += SLOTS) {
+          const int r = rel[a];
+          const T v = cbr[at32(g, L.sumcbr, cr.cbr_off + a, lane)];
+          if (r < w) PE(r, f) += v;
+          else if (trail) CR(r - w) += v;
+        }
+      __syncthreads();
+    }
+    // LU of the panel, one pivot per barrier: rows p < i < w over columns p < j < ncols
+    // (top part) and rows i >= w over columns p < j < w (left part), each entry with
+    // the unscaled l_ip = F(i,p) / F(p,p) of its row; column p is scaled one pivot later
+    // (and after the loop for the last pivot), when no thread reads it any more
+    T inv_prev = (T)1;
+    for (int p = 0; p < w; ++p) {
+      T pk = PE(p, p);
+      if (bad_pivot(pk)) {
+        if (slot == 0) mark_singular(&status[g * 32 + lane]);
+        pk = (T)1;
+      }
+      const T inv = (T)1 / pk;
+      if (p > 0)
+        for (int i = p + slot; i < f; i += SLOTS) PE(i, p - 1) *= inv_prev;
+      const int nt = (w - 1 - p) * (ncols - 1 - p);  // top part: rows p+1 .. w-1
+      for (int e = slot; e < nt; e += SLOTS) {
+        const int i = p + 1 + e / (ncols - 1 - p), j = p + 1 + e % (ncols - 1 - p);
+        const T lip = PE(i, p) * inv;
+        PE(i, j) = PE(i, j) - lip * PE(p, j);
+      }
+      const int nl = m * (w - 1 - p);  // left part: rows w .. f-1, columns p+1 .. w-1
+      for (int e = slot; e < nl; e += SLOTS) {
+        const int i = w + e / (w - 1 - p), j = p + 1 + e % (w - 1 - p);
+        const T lip = PE(i, p) * inv;
+        PE(i, j) = PE(i, j) - lip * PE(p, j);
+      }
+      inv_prev = inv;
+      __syncthreads();
+    }
+    if (w > 0) {
+      for (int i = w + slot; i < f; i += SLOTS) PE(i, w - 1) *= inv_prev;
+      __syncthreads();
+    }
+    // the Schur complement on the trailing block (and the carried right-hand side):
+    // x - l_ip u_pj in pivot order
+    if (trail) {
+      for (int e = slot; e < m * m; e += SLOTS) {
+        const int a = e / m, b = e % m;
+        T c = CE(a, b);
+        for (int p = 0; p < w; ++p) c = c - PE(w + a, p) * PE(p, w + b);
+        CE(a, b) = c;
+      }
+      if (with_rhs)
+        for (int a = slot; a < m; a += SLOTS) {
+          T c = CR(a);
+          for (int p = 0; p < w; ++p) c = c - PE(w + a, p) * PE(p, f);
+          CR(a) = c;
+        }
+    }
+    // U panel (rows 0 .. w-1, all f columns), L panel (rows w .. f-1, columns 0 .. w-1)
+    T* pb = pan + at32(g, L.nnz, L.pan_off[s], lane);
+    for (int e = slot; e < w * f; e += SLOTS) pb[(size_t)e * 32] = PE(e / f, e % f);
+    for (int e = slot; e < m * w; e += SLOTS) pb[((size_t)w * f + e) * 32] = PE(w + e / w, e % w);
+    if (with_rhs)
+      for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, rows[p], lane)] = PE(p, f);
+    __syncthreads();
+  }
+}
+
 // Forward substitution with stored factors (fast-decoupled solves): thread per
 // case, warp per (supernode, group).  b accumulates in shared memory.
 template <typename T>

@@ -111,6 +111,11 @@ def test_multifrontal_symbolic_by_host_emulation(tmp_path):
             assert out.returncode == 0, out.stdout + out.stderr
             errs = [float(x) for x in out.stdout.split()]
             assert max(errs) < 1e-10
+    # a densely meshed grid (uniform-random topology): 76 fronts above 167 rows take the
+    # panel / trailing-block split of k_mf_factor_big, equal to the dense loop bit for bit
+    out = subprocess.run([str(exe), "1354", "1991", "260", "0", "1"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "big fronts 76, mismatching entries 0" in out.stderr
 
 
 def test_python_binding_reports_no_device_without_gpu():
