@@ -605,7 +605,7 @@ void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const
   CUDA_TRY(cudaGetLastError());
 }
 
-// Fronts too large for a dense front in shared memory: k_mf_factor_big, a 256-thread
+// Fronts too large for a dense front in shared memory: k_mf_factor_big, a 512-thread
 // block per (supernode, chunk of ge lanes), the launch's largest panel in shared memory
 template <typename T>
 void launch_factor_big(int ge, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr,
@@ -617,9 +617,9 @@ void launch_factor_big(int ge, const LUSystem& sys, const Launch& ln, int ngroup
   const DevLU dl = sys.dev();
   const int* ts = sys.lev_sn.as<int>() + ln.offset;
   switch (ge) {
-    case 4: k_mf_factor_big<T, 4><<<blocks, 256, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
-    case 2: k_mf_factor_big<T, 2><<<blocks, 256, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
-    case 1: k_mf_factor_big<T, 1><<<blocks, 256, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    case 4: k_mf_factor_big<T, 4><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    case 2: k_mf_factor_big<T, 2><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    case 1: k_mf_factor_big<T, 1><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
     default: throw MpfError{MPF_ERR_INTERNAL, "no big-front kernel for this lane count"};
   }
   CUDA_TRY(cudaGetLastError());

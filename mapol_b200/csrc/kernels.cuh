@@ -1188,16 +1188,16 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
 // the panel's LU.  Every entry takes the same operations in the same order as in the
 // one-pivot loop of k_mf_factor (assignment of the arrowhead value, the children's
 // additions in child order, then x - l_ip u_pj for p = 0 .. w - 1), so the factors are
-// the same bit for bit.  One 256-thread block per task (supernode, chunk of G lanes);
+// the same bit for bit.  One 512-thread block per task (supernode, chunk of G lanes);
 // thread = (entry slot, lane); dynamic shared memory: the launch's largest panel.
 template <typename T, int G>
-__global__ void __launch_bounds__(256) k_mf_factor_big(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+__global__ void __launch_bounds__(512, 1) k_mf_factor_big(DevLU L, const int* __restrict__ task_sn, int nsn_l,
                                                        int ngroups, const T* __restrict__ A,
                                                        T* __restrict__ pan, T* __restrict__ cb,
                                                        T* __restrict__ cbr, T* __restrict__ x,
                                                        int* __restrict__ status,
                                                        const int* __restrict__ group_active, int with_rhs) {
-  constexpr int SLOTS = 256 / G, LPG = 32 / G;
+  constexpr int SLOTS = 512 / G, LPG = 32 / G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* P = reinterpret_cast<T*>(smem_raw);
   const int slot = threadIdx.x / G, l = threadIdx.x % G;
@@ -1247,11 +1247,28 @@ __global__ void __launch_bounds__(256) k_mf_factor_big(DevLU L, const int* __res
       const ChildRef cr = L.child_ref[ci];
       const int mc = cr.m;
       const int* rel = L.relmap + cr.rel_ptr;
-      for (int e = slot; e < mc * mc; e += SLOTS) {
-        const int r = rel[e / mc], c = rel[e % mc];
-        const T v = cb[at32(g, L.sumcb, cr.cb_off + e, lane)];
-        if (r < w || c < w) PE(r, c) += v;
-        else if (trail) CE(r - w, c - w) += v;
+      // eight entries per thread at a time: all their loads (the child's values and the
+      // trailing entries they add to, distinct within a child) before any store
+      constexpr int B = 8;
+      for (int e0 = slot; e0 < mc * mc; e0 += B * SLOTS) {
+        int r[B], c[B];
+        T v[B], t[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+          const int e = e0 + u * SLOTS;
+          r[u] = e < mc * mc ? rel[e / mc] : 0;
+          c[u] = e < mc * mc ? rel[e % mc] : 0;
+          v[u] = e < mc * mc ? cb[at32(g, L.sumcb, cr.cb_off + e, lane)] : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+          t[u] = (e0 + u * SLOTS < mc * mc && r[u] >= w && c[u] >= w && trail) ? CE(r[u] - w, c[u] - w) : (T)0;
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+          if (e0 + u * SLOTS >= mc * mc) break;
+          if (r[u] < w || c[u] < w) PE(r[u], c[u]) += v[u];
+          else if (trail) CE(r[u] - w, c[u] - w) = t[u] + v[u];
+        }
       }
       if (with_rhs)
         for (int a = slot; a < mc; a += SLOTS) {
@@ -1276,18 +1293,29 @@ __global__ void __launch_bounds__(256) k_mf_factor_big(DevLU L, const int* __res
       const T inv = (T)1 / pk;
       if (p > 0)
         for (int i = p + slot; i < f; i += SLOTS) PE(i, p - 1) *= inv_prev;
-      const int nt = (w - 1 - p) * (ncols - 1 - p);  // top part: rows p+1 .. w-1
-      for (int e = slot; e < nt; e += SLOTS) {
-        const int i = p + 1 + e / (ncols - 1 - p), j = p + 1 + e % (ncols - 1 - p);
-        const T lip = PE(i, p) * inv;
-        PE(i, j) = PE(i, j) - lip * PE(p, j);
-      }
-      const int nl = m * (w - 1 - p);  // left part: rows w .. f-1, columns p+1 .. w-1
-      for (int e = slot; e < nl; e += SLOTS) {
-        const int i = w + e / (w - 1 - p), j = p + 1 + e % (w - 1 - p);
-        const T lip = PE(i, p) * inv;
-        PE(i, j) = PE(i, j) - lip * PE(p, j);
-      }
+      // four entries per thread at a time, loads before stores: the updated entries
+      // (i > p, j > p) are distinct and none of them is in row p or column p, which the
+      // updates read
+      auto update = [&](int n, int row0, int rowlen) {
+        for (int e0 = slot; e0 < n; e0 += 4 * SLOTS) {
+          int ii[4], jj[4];
+          T lp[4], up[4], b[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int e = min(e0 + u * SLOTS, n - 1);
+            ii[u] = row0 + e / rowlen;
+            jj[u] = p + 1 + e % rowlen;
+            lp[u] = PE(ii[u], p);
+            up[u] = PE(p, jj[u]);
+            b[u] = PE(ii[u], jj[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (e0 + u * SLOTS < n) PE(ii[u], jj[u]) = b[u] - (lp[u] * inv) * up[u];
+        }
+      };
+      update((w - 1 - p) * (ncols - 1 - p), p + 1, ncols - 1 - p);  // top part: rows p+1 .. w-1
+      update(m * (w - 1 - p), w, w - 1 - p);                        // left part: rows w .. f-1
       inv_prev = inv;
       __syncthreads();
     }
@@ -1298,11 +1326,32 @@ __global__ void __launch_bounds__(256) k_mf_factor_big(DevLU L, const int* __res
     // the Schur complement on the trailing block (and the carried right-hand side):
     // x - l_ip u_pj in pivot order
     if (trail) {
-      for (int e = slot; e < m * m; e += SLOTS) {
-        const int a = e / m, b = e % m;
-        T c = CE(a, b);
-        for (int p = 0; p < w; ++p) c = c - PE(w + a, p) * PE(p, w + b);
-        CE(a, b) = c;
+      // 4 x 4 tiles of the trailing block per thread: per pivot, four l and four u
+      // values from shared memory feed sixteen multiply-adds
+      const int nt = (m + 3) / 4;
+      for (int t = slot; t < nt * nt; t += SLOTS) {
+        const int a0 = (t / nt) * 4, b0 = (t % nt) * 4;
+        T acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = (a0 + i < m && b0 + j < m) ? CE(a0 + i, b0 + j) : (T)0;
+        for (int p = 0; p < w; ++p) {
+          T lv[4], uv[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) lv[i] = a0 + i < m ? PE(w + a0 + i, p) : (T)0;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) uv[j] = b0 + j < m ? PE(p, w + b0 + j) : (T)0;
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = acc[i][j] - lv[i] * uv[j];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (a0 + i < m && b0 + j < m) CE(a0 + i, b0 + j) = acc[i][j];
       }
       if (with_rhs)
         for (int a = slot; a < m; a += SLOTS) {

@@ -79,6 +79,10 @@ WORKLOADS = {
     "cfg2_2869bus": dict(n_bus=2869, n_branch=4582, n_pv=509, tap_fraction=0.10, n_out=400, with_base=False),
     "cfg3_9241bus": dict(n_bus=9241, n_branch=16049, n_pv=1445, tap_fraction=0.15, n_out=1000, with_base=False),
     "cfg4_1354bus": dict(n_bus=1354, n_branch=1991, n_pv=259, tap_fraction=0.10, n_out=0, with_base=False),
+    # stress row: the same sizes with uniform-random extra branches (topology 1), a
+    # densely meshed grid whose fronts reach 337 rows (large-front kernel)
+    "stress_uniform_1354bus": dict(n_bus=1354, n_branch=1991, n_pv=259, tap_fraction=0.10, n_out=1000,
+                                   with_base=False, topology=1),
 }
 
 
@@ -90,7 +94,8 @@ def workload(name, seed=1, outage_seed=7):
     """(buses, branches, cases) of a named workload.  The N-1 set holds n_out
     non-bridge outages, or every non-bridge branch when the grid has fewer."""
     w = WORKLOADS[name]
-    buses, branches = synth_grid(w["n_bus"], w["n_branch"], w["n_pv"], w["tap_fraction"], seed=seed)
+    buses, branches = synth_grid(w["n_bus"], w["n_branch"], w["n_pv"], w["tap_fraction"], seed=seed,
+                                 topology=w.get("topology", 0))
     n_out = w["n_out"]
     if n_out:
         n_out = min(n_out, int((find_bridges(branches, w["n_bus"]) == 0).sum()))
