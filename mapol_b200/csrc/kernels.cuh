@@ -1250,15 +1250,20 @@ __global__ void __launch_bounds__(512, 1) k_mf_factor_big(DevLU L, const int* __
       // eight entries per thread at a time: all their loads (the child's values and the
       // trailing entries they add to, distinct within a child) before any store
       constexpr int B = 8;
+      // entry e = a mc + b of the child's block; (a, b) advance by SLOTS without divisions
+      const int sa = SLOTS / mc, sb = SLOTS % mc;
+      int a = slot / mc, b = slot % mc;
+      const T* src = cb + at32(g, L.sumcb, cr.cb_off, lane);
       for (int e0 = slot; e0 < mc * mc; e0 += B * SLOTS) {
         int r[B], c[B];
         T v[B], t[B];
 #pragma unroll
         for (int u = 0; u < B; ++u) {
           const int e = e0 + u * SLOTS;
-          r[u] = e < mc * mc ? rel[e / mc] : 0;
-          c[u] = e < mc * mc ? rel[e % mc] : 0;
-          v[u] = e < mc * mc ? cb[at32(g, L.sumcb, cr.cb_off + e, lane)] : (T)0;
+          r[u] = e < mc * mc ? rel[a] : 0;
+          c[u] = e < mc * mc ? rel[b] : 0;
+          v[u] = e < mc * mc ? src[(size_t)e * 32] : (T)0;
+          next_task(a, b, sa, sb, mc);
         }
 #pragma unroll
         for (int u = 0; u < B; ++u)
@@ -1296,26 +1301,37 @@ __global__ void __launch_bounds__(512, 1) k_mf_factor_big(DevLU L, const int* __
       // four entries per thread at a time, loads before stores: the updated entries
       // (i > p, j > p) are distinct and none of them is in row p or column p, which the
       // updates read
-      auto update = [&](int n, int row0, int rowlen) {
+      // rows of the part start at `base` (shared-memory index of column 0 of its first
+      // row, row stride rstride entries); entry e = i rowlen + j' of the part is row i,
+      // column p + 1 + j'; (i, j') advance by SLOTS without divisions
+      auto update = [&](int n, int base, int rstride, int rowlen) {
+        if (n <= 0) return;
+        const int si = SLOTS / rowlen, sj = SLOTS % rowlen;
+        int i = slot / rowlen, j = slot % rowlen;
+        const T* prow = P + ((size_t)p * (f + 1) + p + 1) * G + l;  // u_pj, j > p
         for (int e0 = slot; e0 < n; e0 += 4 * SLOTS) {
-          int ii[4], jj[4];
-          T lp[4], up[4], b[4];
+          int at[4], jc[4];
+          T lp[4], up[4], bv[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const int e = min(e0 + u * SLOTS, n - 1);
-            ii[u] = row0 + e / rowlen;
-            jj[u] = p + 1 + e % rowlen;
-            lp[u] = PE(ii[u], p);
-            up[u] = PE(p, jj[u]);
-            b[u] = PE(ii[u], jj[u]);
+            const bool ok = e0 + u * SLOTS < n;
+            const int row = base + (ok ? i : 0) * rstride;
+            at[u] = row + p + 1 + (ok ? j : 0);
+            jc[u] = ok ? j : 0;
+            lp[u] = P[(size_t)(row + p) * G + l];
+            up[u] = prow[(size_t)jc[u] * G];
+            bv[u] = P[(size_t)at[u] * G + l];
+            next_task(i, j, si, sj, rowlen);
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u)
-            if (e0 + u * SLOTS < n) PE(ii[u], jj[u]) = b[u] - (lp[u] * inv) * up[u];
+            if (e0 + u * SLOTS < n) P[(size_t)at[u] * G + l] = bv[u] - (lp[u] * inv) * up[u];
         }
       };
-      update((w - 1 - p) * (ncols - 1 - p), p + 1, ncols - 1 - p);  // top part: rows p+1 .. w-1
-      update(m * (w - 1 - p), w, w - 1 - p);                        // left part: rows w .. f-1
+      // top part: rows p+1 .. w-1, columns p+1 .. ncols-1
+      update((w - 1 - p) * (ncols - 1 - p), (p + 1) * (f + 1), f + 1, ncols - 1 - p);
+      // left part: rows w .. f-1, columns p+1 .. w-1
+      update(m * (w - 1 - p), w * (f + 1), w, w - 1 - p);
       inv_prev = inv;
       __syncthreads();
     }
@@ -1336,12 +1352,15 @@ __global__ void __launch_bounds__(512, 1) k_mf_factor_big(DevLU L, const int* __
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) acc[i][j] = (a0 + i < m && b0 + j < m) ? CE(a0 + i, b0 + j) : (T)0;
+        // l of rows w + a0 + i (left part, stride w) and u of columns w + b0 + j (top part)
+        const T* lb = P + ((size_t)w * (f + 1) + (size_t)a0 * w) * G + l;
+        const T* ub = P + (size_t)(w + b0) * G + l;
         for (int p = 0; p < w; ++p) {
           T lv[4], uv[4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) lv[i] = a0 + i < m ? PE(w + a0 + i, p) : (T)0;
+          for (int i = 0; i < 4; ++i) lv[i] = a0 + i < m ? lb[((size_t)i * w + p) * G] : (T)0;
 #pragma unroll
-          for (int j = 0; j < 4; ++j) uv[j] = b0 + j < m ? PE(p, w + b0 + j) : (T)0;
+          for (int j = 0; j < 4; ++j) uv[j] = b0 + j < m ? ub[((size_t)p * (f + 1) + j) * G] : (T)0;
 #pragma unroll
           for (int i = 0; i < 4; ++i)
 #pragma unroll
