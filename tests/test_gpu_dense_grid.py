@@ -63,3 +63,54 @@ def test_dense_grid_kernels_agree_bit_for_bit(dense_grid):
             pf.solve(m.NR, m.MIXED)
             out.append(pf.results().v)
     assert np.array_equal(out[0], out[1])
+
+
+def test_dense_grid_adjoint_matches_finite_differences(gpu):
+    """The adjoint on the dense grid: its transposed substitutions run on the large
+    fronts' factors with fewer warps per block (a warp's slice of x of a 352-row front
+    takes 86 KB in FP64).  Injection gradients against central FP64 differences (step
+    1e-6, the tolerance of tests/test_gpu_adjoint.py), and the refined FP32-factor
+    adjoint against the FP64 one."""
+    tol, h = 1e-12, 1e-6
+    buses, branches = m.synth_grid(1354, 1991, 260, tap_fraction=0.05, seed=5, topology=1)
+    cases = [[]] + m.n1_cases(branches, len(buses), 7, 3)
+
+    def loss(rating, sbus=None):
+        with m.PowerFlow(buses, branches, tol=tol) as pf:
+            pf.set_cases(cases, sbus=sbus)
+            pf.solve(m.NR, m.FP64)
+            assert (pf.results().status == m.runpf.CONVERGED).all()
+            pf.set_ratings(rating)
+            return pf.branch_flows()["overload"]
+
+    with m.PowerFlow(buses, branches, tol=tol) as pf:
+        pf.set_cases(cases)
+        pf.solve(m.NR, m.FP64)
+        rating = 1.2 * np.abs(pf.branch_flows(flows=True)["sf"][0])
+        pf.set_ratings(rating)
+        L = pf.branch_flows()["overload"]
+        g64 = pf.adjoint(m.FP64)
+        g32 = pf.adjoint(m.MIXED)
+    assert (L > 0).any()
+    s0 = np.stack([np.tile(buses["p"], (len(cases), 1)), np.tile(buses["q"], (len(cases), 1))], -1)
+    # PQ buses with gradients well above the differences' noise floor (~5e-10): three of
+    # the twenty largest in P and in Q
+    pq = np.where(buses["type"] == 1)[0]
+    rng = np.random.default_rng(4)
+    coords = []
+    for comp, key in ((0, "grad_p"), (1, "grad_q")):
+        top = pq[np.argsort(-np.abs(g64[key][:, pq]).max(0))[:20]]
+        coords += [(int(i), comp) for i in rng.choice(top, 3, replace=False)]
+    adjs, fds = [], []
+    for i, comp in coords:
+        sp, sm = s0.copy(), s0.copy()
+        sp[:, i, comp] += h
+        sm[:, i, comp] -= h
+        fds.append((loss(rating, sp) - loss(rating, sm)) / (2 * h))
+        adjs.append((g64["grad_p"] if comp == 0 else g64["grad_q"])[:, i])
+    adj, fd = np.concatenate(adjs), np.concatenate(fds)
+    assert np.linalg.norm(adj - fd) <= 1e-6 * np.linalg.norm(fd), (np.linalg.norm(adj - fd), np.linalg.norm(fd))
+    assert (np.abs(adj - fd) <= 1e-5 * np.abs(fd) + 2e-9).all()
+    for key in ("grad_p", "grad_q", "grad_g", "grad_b"):
+        a, b = g64[key], g32[key]
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max() + 1e-15, (key, np.abs(a - b).max())
