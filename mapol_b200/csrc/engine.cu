@@ -99,9 +99,10 @@ inline size_t big_panel(int w, int f) { return (size_t)w * (2 * f - w + 1); }
 inline std::string front_limits(const LUSymbolic& L, const char* what) {
   for (int s = 0; s < L.nsn; ++s) {
     const int w = L.sn_w[s], f = L.sn_f[s];
-    if (f > kFmaxAll && big_panel(w, f) * 8 > kSmemMax)
+    if (f > kFmaxAll && (big_panel(w, f) + (f - w + 1)) * 8 > kSmemMax)
       return std::string(what) + ": a front of " + std::to_string(f) + " rows with " + std::to_string(w) +
-             " pivots needs a " + std::to_string(big_panel(w, f) * 8 / 1024) + " KB panel, above the " +
+             " pivots needs a " + std::to_string((big_panel(w, f) + (f - w + 1)) * 8 / 1024) +
+             " KB panel and trailing row, above the " +
              std::to_string(kSmemMax / 1024) + " KB of shared memory (grid too densely meshed)";
     if ((size_t)f * 32 * 8 > kSmemMax)
       return std::string(what) + ": a front of " + std::to_string(f) + " rows exceeds " +
@@ -133,6 +134,7 @@ struct Launch {
   int wfmax = 0;                 // largest w * f in range (U-panel entries)
   int level = 0;                 // elimination-tree level
   size_t pcap = 0;               // CLS_BIG: largest panel in range, w (2f - w + 1) entries
+  int mcap = 0;                  // CLS_BIG: largest trailing block in range, m = f - w rows
 };
 
 // Side streams of one LU system, created on first use.  The factorisation's launches
@@ -352,7 +354,10 @@ struct LUSystem {
     for (Launch& ln : factor_sched)
       if (ln.cls == CLS_BIG)
         for (int t = ln.offset; t < ln.offset + ln.count; ++t)
+        {
           ln.pcap = std::max(ln.pcap, big_panel(s.sn_w[s.lev_sn[t]], s.sn_f[s.lev_sn[t]]));
+          ln.mcap = std::max(ln.mcap, s.sn_f[s.lev_sn[t]] - s.sn_w[s.lev_sn[t]]);
+        }
     for (const Launch& ln : factor_sched) {
       fingerprint = (fingerprint ^ (uint64_t)ln.offset) * 1099511628211ull;
       fingerprint = (fingerprint ^ (uint64_t)ln.count) * 1099511628211ull;
@@ -576,6 +581,9 @@ void ensure_attrs(int device) {
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big_gt<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big_gt<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+  CUDA_TRY(cudaFuncSetAttribute(k_mf_factor_big_gt<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
   CUDA_TRY(cudaFuncSetAttribute(k_mf_bsolve_top<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
@@ -606,10 +614,31 @@ void launch_factor_one(const LUSystem& sys, const Launch& ln, int ngroups, const
 }
 
 // Fronts too large for a dense front in shared memory: k_mf_factor_big, a 512-thread
-// block per (supernode, chunk of ge lanes), the launch's largest panel in shared memory
+// block per (supernode, chunk of ge lanes); shared memory holds the launch's largest
+// panel and a slab of S trailing rows of its largest trailing block
 template <typename T>
-void launch_factor_big(int ge, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb, T* cbr,
-                       T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
+void launch_factor_big(int ge, int S, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb,
+                       T* cbr, T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
+  const size_t smem = (ln.pcap + (size_t)S * (ln.mcap + 1)) * ge * sizeof(T);
+  if (ln.pcap == 0 || S < 1 || smem > kSmemMax) throw MpfError{MPF_ERR_INTERNAL, "big-front panel does not fit"};
+  const long long ntasks = (long long)ln.count * ngroups * (32 / ge);
+  const unsigned blocks = (unsigned)std::min<long long>(ntasks, 148LL * 32);
+  const DevLU dl = sys.dev();
+  const int* ts = sys.lev_sn.as<int>() + ln.offset;
+  switch (ge) {
+    case 4: k_mf_factor_big<T, 4><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, (int)ln.pcap, S); break;
+    case 2: k_mf_factor_big<T, 2><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, (int)ln.pcap, S); break;
+    case 1: k_mf_factor_big<T, 1><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, (int)ln.pcap, S); break;
+    default: throw MpfError{MPF_ERR_INTERNAL, "no big-front kernel for this lane count"};
+  }
+  CUDA_TRY(cudaGetLastError());
+}
+
+// The large-front variant with the trailing block in global memory (kind 7): only the
+// launch's largest panel in shared memory
+template <typename T>
+void launch_factor_big_gt(int ge, const LUSystem& sys, const Launch& ln, int ngroups, const T* A, T* pan, T* cb,
+                          T* cbr, T* x, int* status, const int* group_active, int with_rhs, cudaStream_t st) {
   const size_t smem = ln.pcap * ge * sizeof(T);
   if (ln.pcap == 0 || smem > kSmemMax) throw MpfError{MPF_ERR_INTERNAL, "big-front panel does not fit"};
   const long long ntasks = (long long)ln.count * ngroups * (32 / ge);
@@ -617,9 +646,9 @@ void launch_factor_big(int ge, const LUSystem& sys, const Launch& ln, int ngroup
   const DevLU dl = sys.dev();
   const int* ts = sys.lev_sn.as<int>() + ln.offset;
   switch (ge) {
-    case 4: k_mf_factor_big<T, 4><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
-    case 2: k_mf_factor_big<T, 2><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
-    case 1: k_mf_factor_big<T, 1><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    case 4: k_mf_factor_big_gt<T, 4><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    case 2: k_mf_factor_big_gt<T, 2><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
+    case 1: k_mf_factor_big_gt<T, 1><<<blocks, 512, smem, st>>>(dl, ts, ln.count, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs); break;
     default: throw MpfError{MPF_ERR_INTERNAL, "no big-front kernel for this lane count"};
   }
   CUDA_TRY(cudaGetLastError());
@@ -696,6 +725,15 @@ inline size_t factor_smem_rt(int fcap, int ge, int teams, int tt, size_t wsize) 
   return b;
 }
 
+// Rows of the trailing block a large-front task of ge lanes holds in shared memory
+// beside the launch's largest panel (0: the panel alone does not fit)
+template <typename T>
+int big_slab_rows(const Launch& ln, int ge) {
+  const size_t cap = kSmemMax / (ge * sizeof(T));
+  if (cap <= ln.pcap) return 0;
+  return (int)std::min<size_t>((cap - ln.pcap) / ((size_t)ln.mcap + 1), (size_t)std::max(ln.mcap, 1));
+}
+
 // The fixed rule (used without autotuning, and as the first candidate): thread per
 // case for fronts up to 8, warp teams up to 24, 256-thread teams above (register
 // LU up to 16 kRegTTMax - 1 rows); lane chunks shrink while a level has too few
@@ -705,10 +743,18 @@ FactorChoice heuristic_choice(const Launch& ln, int ngroups) {
   constexpr int G = Prec<T>::G;
   const long long lanes_tasks = (long long)ln.count * ngroups;
   if (ln.cls == CLS_BIG) {
-    // panels in shared memory: as many lanes per task as the largest panel allows
-    int ge = std::min(G, 4);
-    while (ge > 1 && ln.pcap * ge * sizeof(T) > kSmemMax) ge /= 2;
-    return {6, ge, 0, 1};
+    // the panel and a slab of S trailing rows in shared memory: as many lanes per task
+    // as leave room for slabs of 12 rows (or the whole trailing block), else one lane
+    // with the largest slab that fits (S in the tile field)
+    for (int ge = std::min(G, 4); ge >= 1; ge /= 2) {
+      const int S = big_slab_rows<T>(ln, ge);
+      if (S >= std::min(ln.mcap, 12) && S >= 1) return {6, ge, S, 1};
+      if (ge == 1) {
+        if (S < 1) throw MpfError{MPF_ERR_INTERNAL, "a large front's panel and one trailing row exceed shared memory"};
+        return {6, 1, S, 1};
+      }
+    }
+    throw MpfError{MPF_ERR_INTERNAL, "a large front's panel exceeds shared memory"};
   }
   if (ln.cls == CLS_S && lanes_tasks < kMinWarpTasks) return {1, 32, 0, 1};
   if ((ln.cls == CLS_M1 || ln.cls == CLS_M) && lanes_tasks * (32 / G) < kMinWarpTasks) {
@@ -733,7 +779,22 @@ std::vector<FactorChoice> factor_candidates(const Launch& ln, int ngroups) {
   constexpr int G = Prec<T>::G;
   const size_t ws = sizeof(T);
   std::vector<FactorChoice> c{heuristic_choice<T>(ln, ngroups)};
-  if (ln.cls == CLS_BIG) return c;  // one kernel holds fronts of this size
+  if (ln.cls == CLS_BIG) {
+    // the large-front kernel at each lane count whose panel and a trailing row fit,
+    // with the largest slab beside the panel
+    for (int ge = std::min(Prec<T>::G, 4); ge >= 1; ge /= 2) {
+      const int S = big_slab_rows<T>(ln, ge);
+      if (S >= 1) {
+        const FactorChoice x{6, ge, S, 1};
+        bool dup = false;
+        for (const auto& y : c) dup = dup || (y.kind == x.kind && y.ge == x.ge && y.tt == x.tt);
+        if (!dup) c.push_back(x);
+      }
+      // the trailing block in global memory instead: only the panel in shared memory
+      if (ln.pcap * ge * sizeof(T) <= kSmemMax) c.push_back({7, ge, 0, 1});
+    }
+    return c;
+  }
   auto add = [&](FactorChoice x) {
     for (const auto& y : c)
       if (y.kind == x.kind && y.ge == x.ge && y.tt == x.tt && y.tpb == x.tpb) return;
@@ -796,7 +857,9 @@ void launch_choice(const FactorChoice& ch, const LUSystem& sys, const Launch& ln
   } else if (ch.kind == 2) {
     launch_factor_reg<T>(ch.ge, ch.tt, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
   } else if (ch.kind == 6) {
-    launch_factor_big<T>(ch.ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+    launch_factor_big<T>(ch.ge, ch.tt, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
+  } else if (ch.kind == 7) {
+    launch_factor_big_gt<T>(ch.ge, sys, ln, ngroups, A, pan, cb, cbr, x, status, group_active, with_rhs, st);
   } else if (ch.kind == 5) {
     const bool wide = ch.tpb == 2;
     if (ch.ge == G && wide)

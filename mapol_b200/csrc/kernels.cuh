@@ -598,6 +598,17 @@ __device__ __forceinline__ void next_task(int& q, int& r, int sq, int sr, int nc
   }
 }
 
+// First index a < n with rel[a] >= v (rel increasing), or n
+__device__ __forceinline__ int first_at_least(const int* rel, int n, int v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (rel[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <int TEAM>
 __device__ __forceinline__ void team_sync() {
   if (TEAM == 32) __syncwarp();
@@ -1179,19 +1190,270 @@ __global__ void __launch_bounds__(TEAM == 32 ? 288 : TEAM, TT > 0 ? 2 : (TEAM > 
   }
 }
 
-// Fronts too large for a dense front in shared memory (densely meshed grids).  Only
-// the panel lives in shared memory: the w pivot rows with all f columns and the
-// right-hand side (top part, w x (f + 1)) and the pivot columns of the other rows (left
-// part, m x w, m = f - w), G lanes per entry.  The trailing m x m block is the
-// supernode's contribution block itself, in global memory: zeroed, the children's
-// entries added into it where they fall, and the Schur complement applied there after
-// the panel's LU.  Every entry takes the same operations in the same order as in the
-// one-pivot loop of k_mf_factor (assignment of the arrowhead value, the children's
+// Fronts too large for a dense front in shared memory (densely meshed grids).  The
+// panel stays in shared memory for the whole task: the w pivot rows with all f columns
+// and the right-hand side (top part, w x (f + 1)) and the pivot columns of the other
+// rows (left part, m x w, m = f - w), G lanes per entry.  The trailing m x m block
+// follows in slabs of S rows (shared memory after the panel), each assembled from the
+// children, updated by the Schur complement and written to the supernode's
+// contribution block.  Every entry takes the same operations in the same order as in
+// the one-pivot loop of k_mf_factor (assignment of the arrowhead value, the children's
 // additions in child order, then x - l_ip u_pj for p = 0 .. w - 1), so the factors are
 // the same bit for bit.  One 512-thread block per task (supernode, chunk of G lanes);
-// thread = (entry slot, lane); dynamic shared memory: the launch's largest panel.
+// thread = (entry slot, lane); dynamic shared memory: pcap panel entries (the launch's
+// largest panel) and S (mcap + 1) slab entries (mcap: its largest m), G lanes each.
 template <typename T, int G>
 __global__ void __launch_bounds__(512, 1) k_mf_factor_big(DevLU L, const int* __restrict__ task_sn, int nsn_l,
+                                                       int ngroups, const T* __restrict__ A,
+                                                       T* __restrict__ pan, T* __restrict__ cb,
+                                                       T* __restrict__ cbr, T* __restrict__ x,
+                                                       int* __restrict__ status,
+                                                       const int* __restrict__ group_active, int with_rhs,
+                                                       int pcap, int S) {
+  constexpr int SLOTS = 512 / G, LPG = 32 / G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* P = reinterpret_cast<T*>(smem_raw);
+  const int slot = threadIdx.x / G, l = threadIdx.x % G;
+  const int nch = ngroups * LPG;
+  for (int q = blockIdx.x / nch, ch = blockIdx.x % nch; q < nsn_l;
+       next_task(q, ch, (int)gridDim.x / nch, (int)gridDim.x % nch, nch)) {
+    const int s = task_sn[q];
+    const int g = ch / LPG;
+    if (!group_active[g] || !task_here(L, s, g)) continue;  // uniform over the block
+    const int lane = (ch % LPG) * G + l;
+    const int w = L.sn_w[s], f = L.sn_f[s], m = f - w;
+    const int* rows = L.sn_rows + L.sn_rptr[s];
+    const int RS = front_stride(f);
+    const int ncols = with_rhs ? f + 1 : f;
+    const bool has_parent = L.sn_parent[s] >= 0;
+    const long long cbo = L.cb_off[s], cbro = L.cbr_off[s];
+    const int npan = w * (f + 1) + m * w;
+    // panel entry (r, c), r < w or c < w: top part row-major, then the left part
+    auto PE = [&](int r, int c) -> T& {
+      return r < w ? P[((size_t)r * (f + 1) + c) * G + l] : P[((size_t)w * (f + 1) + (size_t)(r - w) * w + c) * G + l];
+    };
+    // trailing entry (a, b) of the contribution block, and the carried right-hand side
+    auto CE = [&](int a, int b) -> T& { return cb[at32(g, L.sumcb, cbo + (long long)a * m + b, lane)]; };
+    auto CR = [&](int a) -> T& { return cbr[at32(g, L.sumcbr, cbro + a, lane)]; };
+    for (int e = slot; e < npan; e += SLOTS) P[(size_t)e * G + l] = (T)0;
+    __syncthreads();
+    // the arrowhead: pivot rows and pivot columns, all in the panel
+    {
+      const int e0 = L.ah_ptr[s], e1 = L.ah_ptr[s + 1];
+      for (int e = e0 + slot; e < e1; e += SLOTS) {
+        const int loc = L.ah_loc[e];
+        PE(loc / RS, loc % RS) = A[at32(g, L.nA, e, lane)];
+      }
+      if (with_rhs)
+        for (int p = slot; p < w; p += SLOTS) PE(p, f) = x[at32(g, L.n, rows[p], lane)];
+    }
+    __syncthreads();
+    // The children's entries that fall in the panel, one child after the other
+    // (siblings may add into the same entries; within a child the relative map is
+    // injective).  A child's rows map in increasing order, so those landing in pivot
+    // rows are its first aw rows, and its first aw columns land in pivot columns: the
+    // panel takes rows a < aw (all columns) and, of the other rows, columns b < aw.  The
+    // rest goes to the trailing block, slab by slab, after the panel's LU.
+    for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
+      const ChildRef cr = L.child_ref[ci];
+      const int mc = cr.m;
+      const int* rel = L.relmap + cr.rel_ptr;
+      const int aw = first_at_least(rel, mc, w);
+      const T* src = cb + at32(g, L.sumcb, cr.cb_off, lane);
+      // entries (a_first + i, j), i rowlen + j < n, eight per thread at a time (their
+      // loads before their stores); (i, j) advance by SLOTS without divisions
+      auto add_panel = [&](int n, int a_first, int rowlen) {
+        if (n <= 0) return;
+        const int si = SLOTS / rowlen, sj = SLOTS % rowlen;
+        int i = slot / rowlen, j = slot % rowlen;
+        for (int e0 = slot; e0 < n; e0 += 8 * SLOTS) {
+          int r[8], c[8];
+          T v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const bool ok = e0 + u * SLOTS < n;
+            const int a = a_first + (ok ? i : 0), b = ok ? j : 0;
+            r[u] = rel[a];
+            c[u] = rel[b];
+            v[u] = ok ? src[((size_t)a * mc + b) * 32] : (T)0;
+            next_task(i, j, si, sj, rowlen);
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (e0 + u * SLOTS < n) PE(r[u], c[u]) += v[u];
+        }
+      };
+      add_panel(aw * mc, 0, mc);              // rows landing in pivot rows
+      add_panel((mc - aw) * aw, aw, aw);      // the other rows' pivot columns
+      if (with_rhs)
+        for (int a = slot; a < aw; a += SLOTS) PE(rel[a], f) += cbr[at32(g, L.sumcbr, cr.cbr_off + a, lane)];
+      __syncthreads();
+    }
+    // LU of the panel, one pivot per barrier: rows p < i < w over columns p < j < ncols
+    // (top part) and rows i >= w over columns p < j < w (left part), each entry with
+    // the unscaled l_ip = F(i,p) / F(p,p) of its row; column p is scaled one pivot later
+    // (and after the loop for the last pivot), when no thread reads it any more
+    T inv_prev = (T)1;
+    for (int p = 0; p < w; ++p) {
+      T pk = PE(p, p);
+      if (bad_pivot(pk)) {
+        if (slot == 0) mark_singular(&status[g * 32 + lane]);
+        pk = (T)1;
+      }
+      const T inv = (T)1 / pk;
+      if (p > 0)
+        for (int i = p + slot; i < f; i += SLOTS) PE(i, p - 1) *= inv_prev;
+      // four entries per thread at a time, loads before stores: the updated entries
+      // (i > p, j > p) are distinct and none of them is in row p or column p, which the
+      // updates read
+      // rows of the part start at `base` (shared-memory index of column 0 of its first
+      // row, row stride rstride entries); entry e = i rowlen + j' of the part is row i,
+      // column p + 1 + j'; (i, j') advance by SLOTS without divisions
+      auto update = [&](int n, int base, int rstride, int rowlen) {
+        if (n <= 0) return;
+        const int si = SLOTS / rowlen, sj = SLOTS % rowlen;
+        int i = slot / rowlen, j = slot % rowlen;
+        const T* prow = P + ((size_t)p * (f + 1) + p + 1) * G + l;  // u_pj, j > p
+        for (int e0 = slot; e0 < n; e0 += 4 * SLOTS) {
+          int at[4], jc[4];
+          T lp[4], up[4], bv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const bool ok = e0 + u * SLOTS < n;
+            const int row = base + (ok ? i : 0) * rstride;
+            at[u] = row + p + 1 + (ok ? j : 0);
+            jc[u] = ok ? j : 0;
+            lp[u] = P[(size_t)(row + p) * G + l];
+            up[u] = prow[(size_t)jc[u] * G];
+            bv[u] = P[(size_t)at[u] * G + l];
+            next_task(i, j, si, sj, rowlen);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (e0 + u * SLOTS < n) P[(size_t)at[u] * G + l] = bv[u] - (lp[u] * inv) * up[u];
+        }
+      };
+      // top part: rows p+1 .. w-1, columns p+1 .. ncols-1
+      update((w - 1 - p) * (ncols - 1 - p), (p + 1) * (f + 1), f + 1, ncols - 1 - p);
+      // left part: rows w .. f-1, columns p+1 .. w-1
+      update(m * (w - 1 - p), w * (f + 1), w, w - 1 - p);
+      inv_prev = inv;
+      __syncthreads();
+    }
+    if (w > 0) {
+      for (int i = w + slot; i < f; i += SLOTS) PE(i, w - 1) *= inv_prev;
+      __syncthreads();
+    }
+    // The trailing block (and the carried right-hand side as its column m), S rows at a
+    // time in shared memory after the panel: zeroed, given the children's entries that
+    // fall in those rows (a child's rows map in increasing order, so they are one range
+    // of its rows), updated by the Schur complement x - l_ip u_pj in pivot order (4 x 4
+    // register tiles: four l and four u values per pivot feed sixteen multiply-adds),
+    // then written to the supernode's contribution block.  Every child entry is read
+    // once and every trailing entry written once.
+    if (has_parent && m > 0) {
+      T* Sb = P + (size_t)pcap * G + l;  // slab entry (row, col) at Sb[(row * mcols + col) * G]
+      const int mcols = m + 1;
+      const int bc = with_rhs ? m + 1 : m;  // columns updated and written
+      for (int a0 = 0; a0 < m; a0 += S) {
+        const int sr = min(S, m - a0);
+        for (int e = slot; e < sr * mcols; e += SLOTS) Sb[(size_t)e * G] = (T)0;
+        __syncthreads();
+        for (int ci = L.child_ptr[s]; ci < L.child_ptr[s + 1]; ++ci) {
+          const ChildRef cr = L.child_ref[ci];
+          const int mc = cr.m;
+          const int* rel = L.relmap + cr.rel_ptr;
+          const int aw = first_at_least(rel, mc, w);
+          const int lo = first_at_least(rel, mc, w + a0), hi = first_at_least(rel, mc, w + a0 + sr);
+          const int rowlen = mc - aw, n = (hi - lo) * rowlen;
+          const T* src = cb + at32(g, L.sumcb, cr.cb_off, lane);
+          if (n > 0) {
+            const int si = SLOTS / rowlen, sj = SLOTS % rowlen;
+            int i = slot / rowlen, j = slot % rowlen;
+            for (int e0 = slot; e0 < n; e0 += 8 * SLOTS) {
+              int at[8];
+              T v[8], t[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) {
+                const bool ok = e0 + u * SLOTS < n;
+                const int a = lo + (ok ? i : 0), b = aw + (ok ? j : 0);
+                at[u] = (rel[a] - w - a0) * mcols + (rel[b] - w);
+                v[u] = ok ? src[((size_t)a * mc + b) * 32] : (T)0;
+                t[u] = Sb[(size_t)at[u] * G];
+                next_task(i, j, si, sj, rowlen);
+              }
+#pragma unroll
+              for (int u = 0; u < 8; ++u)
+                if (e0 + u * SLOTS < n) Sb[(size_t)at[u] * G] = t[u] + v[u];
+            }
+          }
+          if (with_rhs)
+            for (int a = lo + slot; a < hi; a += SLOTS)
+              Sb[((size_t)(rel[a] - w - a0) * mcols + m) * G] += cbr[at32(g, L.sumcbr, cr.cbr_off + a, lane)];
+          __syncthreads();
+        }
+        const int nta = (sr + 3) / 4, ntb = (bc + 3) / 4;
+        for (int tt = slot; tt < nta * ntb; tt += SLOTS) {
+          const int ra = (tt / ntb) * 4, b0 = (tt % ntb) * 4;
+          T acc[4][4];
+#pragma unroll
+          for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj)
+              acc[ii][jj] = (ra + ii < sr && b0 + jj < bc) ? Sb[((size_t)(ra + ii) * mcols + b0 + jj) * G] : (T)0;
+          // l of trailing rows a0 + ra + ii (left part, stride w); u of columns w + b0 + jj
+          // (top part; column w + m is the right-hand side f)
+          const T* lb = P + ((size_t)w * (f + 1) + (size_t)(a0 + ra) * w) * G + l;
+          const T* ub = P + (size_t)(w + b0) * G + l;
+          for (int p = 0; p < w; ++p) {
+            T lv[4], uv[4];
+#pragma unroll
+            for (int ii = 0; ii < 4; ++ii) lv[ii] = ra + ii < sr ? lb[((size_t)ii * w + p) * G] : (T)0;
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) uv[jj] = b0 + jj < bc ? ub[((size_t)p * (f + 1) + jj) * G] : (T)0;
+#pragma unroll
+            for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+              for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = acc[ii][jj] - lv[ii] * uv[jj];
+          }
+#pragma unroll
+          for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj)
+              if (ra + ii < sr && b0 + jj < bc) Sb[((size_t)(ra + ii) * mcols + b0 + jj) * G] = acc[ii][jj];
+        }
+        __syncthreads();
+        {
+          const int si = SLOTS / m, sj = SLOTS % m;
+          int i = slot / m, j = slot % m;
+          for (int e = slot; e < sr * m; e += SLOTS) {
+            CE(a0 + i, j) = Sb[((size_t)i * mcols + j) * G];
+            next_task(i, j, si, sj, m);
+          }
+          if (with_rhs)
+            for (int a = slot; a < sr; a += SLOTS) CR(a0 + a) = Sb[((size_t)a * mcols + m) * G];
+        }
+        __syncthreads();
+      }
+    }
+    // U panel (rows 0 .. w-1, all f columns), L panel (rows w .. f-1, columns 0 .. w-1)
+    T* pb = pan + at32(g, L.nnz, L.pan_off[s], lane);
+    for (int e = slot; e < w * f; e += SLOTS) pb[(size_t)e * 32] = PE(e / f, e % f);
+    for (int e = slot; e < m * w; e += SLOTS) pb[((size_t)w * f + e) * 32] = PE(w + e / w, e % w);
+    if (with_rhs)
+      for (int p = slot; p < w; p += SLOTS) x[at32(g, L.n, rows[p], lane)] = PE(p, f);
+    __syncthreads();
+  }
+}
+
+// The same factorisation with the trailing block kept in global memory (the
+// supernode's contribution block, zeroed, the children's entries added into it, the
+// Schur complement applied there after the panel's LU): only the panel takes shared
+// memory, so more lanes fit per task; a tuning candidate beside k_mf_factor_big, whose
+// slabs get short when the panel leaves little shared memory (FP64).  Same operations
+// in the same order, so the same factors bit for bit.
+template <typename T, int G>
+__global__ void __launch_bounds__(512, 1) k_mf_factor_big_gt(DevLU L, const int* __restrict__ task_sn, int nsn_l,
                                                        int ngroups, const T* __restrict__ A,
                                                        T* __restrict__ pan, T* __restrict__ cb,
                                                        T* __restrict__ cbr, T* __restrict__ x,

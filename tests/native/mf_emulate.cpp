@@ -54,6 +54,10 @@ static double solve_check(const LUSymbolic& L, const std::vector<int>& ah_ptr, c
         const int ch = L.child_list[ci];
         const int mm = L.sn_f[ch] - L.sn_w[ch];
         const int* rel = L.relmap.data() + L.rel_ptr[ch];
+        // a child's rows map in increasing order (k_mf_factor_big finds the rows that
+        // fall in pivot rows, and in each trailing slab, as ranges of them)
+        for (int a = 1; a < mm; ++a)
+          if (rel[a] <= rel[a - 1]) { std::printf("relative map not increasing\n"); std::exit(6); }
         for (int idx = 0; idx < mm * mm; ++idx) F[rel[idx / mm] * f1 + rel[idx % mm]] += cb[L.cb_off[ch] + idx];
         if (fused_forward)
           for (int a = 0; a < mm; ++a) F[rel[a] * f1 + f] += cbr[L.cbr_off[ch] + a];
