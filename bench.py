@@ -538,8 +538,9 @@ def run_ours(args, rank, world, local_rank):
                      "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                      "traffic_unit": "DRAM bytes per factorisation of all cases (all its level launches)",
                      "alg_bytes": alg_bytes("factor_ms", 4) * n_cases,
-                     "traffic_source": "ncu dram__bytes_read+write.sum, 256 cases, per case x cases "
-                                       "(profiles/dram_nr_mixed_9241bus_256cases.md)",
+                     "traffic_source": ("ncu dram__bytes_read+write.sum, 256 cases, per case x cases "
+                                        "(profiles/dram_nr_mixed_9241bus_256cases.md)") if traffic is not None
+                                       else None,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                      "per_family": per_family},
         "gpu_launches": int(mixed["launches"]),
