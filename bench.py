@@ -436,6 +436,28 @@ def run_ours(args, rank, world, local_rank):
     clocks = sampler.stop() if sampler else None
     st = pf.stats()  # after the solves: device_bytes includes the factor buffers
 
+    # the same mixed solves with the whole Newton loop as one CUDA graph (use_graph = 2:
+    # a device-side while node instead of one host flag read per iteration)
+    with m.PowerFlow(buses, branches, device=local_rank, use_graph=2) as pf2:
+        pf2.set_cases(cases)
+        for _ in range(args.warmup):
+            pf2.solve(m.NR, m.MIXED, stream.cuda_stream)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            pf2.solve(m.NR, m.MIXED, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_loop = max_over_ranks(e0.elapsed_time(e1))
+        r2 = pf2.results()
+        device_loop = {"value": n_cases * world * args.steps / (ms_loop / 1e3), "unit": "solves/s",
+                       "ms_per_step": ms_loop / args.steps,
+                       "identical_to_host_loop": bool(np.array_equal(r2.v, out["mixed"]["res"].v) and
+                                                      np.array_equal(r2.iterations, out["mixed"]["res"].iterations))}
+
     # end to end through the host C-ABI call: case definitions in from pinned host
     # memory, voltages / flags / iterations / mismatch back into pinned host memory
     e2e = None
@@ -545,6 +567,7 @@ def run_ours(args, rank, world, local_rank):
                      "per_family": per_family},
         "gpu_launches": int(mixed["launches"]),
         "clocks": clocks,
+        "device_loop": device_loop,
     }
     if e2e:
         line["e2e"] = e2e

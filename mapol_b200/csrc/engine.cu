@@ -1489,6 +1489,12 @@ struct mpf_handle {
     const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
     DevGrid dkey;  // the grid descriptor the kernels were captured with
     int ngroups = 0, launches[4] = {0, 0, 0, 0};
+    // use_graph = 2: the whole Newton loop as one graph (a condition kernel, then a
+    // while node whose body is the four parts and the condition kernel again)
+    cudaGraph_t loop_graph = nullptr;
+    cudaGraphExec_t loop_exec = nullptr;
+    int loop_launches = 0;  // launches per body run
+    bool captured(bool dev_loop) const { return dev_loop ? loop_exec != nullptr : exec[0] != nullptr; }
     void release() {
       for (int k = 0; k < 4; ++k) {
         if (exec[k]) cudaGraphExecDestroy(exec[k]);
@@ -1496,6 +1502,10 @@ struct mpf_handle {
         exec[k] = nullptr;
         graph[k] = nullptr;
       }
+      if (loop_exec) cudaGraphExecDestroy(loop_exec);
+      if (loop_graph) cudaGraphDestroy(loop_graph);  // also frees the while node's body
+      loop_exec = nullptr;
+      loop_graph = nullptr;
       ngroups = 0;
     }
   } nr_graph[2];
@@ -1829,22 +1839,58 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
     tune_factor<T>(J, h->ngroups, A, pan, cb, cbr, x, d.status, d.group_active, st);
     tune_bsolve<T>(J, h->ngroups, pan, x, d.group_active, st);
   }
+  const bool dev_loop = h->opt.use_graph == 2;
   if (h->opt.use_graph) {
     // the captured kernels hold every device pointer of d by value: capture again
     // when any of them (or the LU buffers) changed since
     const void* key[4] = {A, pan, cb, x};
-    if (gph.exec[0] && (gph.ngroups != h->ngroups || std::memcmp(gph.key, key, sizeof(key)) != 0 ||
-                        std::memcmp(&gph.dkey, &d, sizeof(d)) != 0))
+    if ((gph.exec[0] || gph.loop_exec) &&
+        (gph.ngroups != h->ngroups || std::memcmp(gph.key, key, sizeof(key)) != 0 ||
+         std::memcmp(&gph.dkey, &d, sizeof(d)) != 0))
       gph.release();
-    if (!gph.exec[0]) {
-      // capture each part on a private stream (the caller's may be the legacy one)
+    if (!gph.captured(dev_loop)) {
+      // capture on a private stream (the caller's may be the legacy one)
       cudaStream_t cs;
       CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-      for (int part = 0; part < 4; ++part) {
-        CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        gph.launches[part] = enqueue_nr_part<T>(h, part, cs, A, pan, cb, cbr, x);
-        CUDA_TRY(cudaStreamEndCapture(cs, &gph.graph[part]));
-        CUDA_TRY(cudaGraphInstantiate(&gph.exec[part], gph.graph[part], 0));
+      if (!dev_loop) {
+        for (int part = 0; part < 4; ++part) {
+          CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+          gph.launches[part] = enqueue_nr_part<T>(h, part, cs, A, pan, cb, cbr, x);
+          CUDA_TRY(cudaStreamEndCapture(cs, &gph.graph[part]));
+          CUDA_TRY(cudaGraphInstantiate(&gph.exec[part], gph.graph[part], 0));
+        }
+      } else {
+        // head: the condition at entry; then a while node running the four parts and
+        // the condition again.  The update kernel counts iterations on the device, so
+        // the loop ends after at most max_it bodies whatever the cases do.
+        CUDA_TRY(cudaGraphCreate(&gph.loop_graph, 0));
+        cudaGraphConditionalHandle hc;
+        CUDA_TRY(cudaGraphConditionalHandleCreate(&hc, gph.loop_graph, 0, 0));
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, gph.loop_graph, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+        k_loop_cond<<<1, 1, 0, cs>>>(hc, h->any_active.as<int>(), d.it_ptr, max_it);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamEndCapture(cs, &gph.loop_graph));
+        cudaGraphNode_t head;
+        size_t nn = 1;
+        CUDA_TRY(cudaGraphGetNodes(gph.loop_graph, &head, &nn));
+        if (nn != 1) throw MpfError{MPF_ERR_CUDA, "device loop: the head graph should hold one kernel"};
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hc;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t loop;
+        CUDA_TRY(cudaGraphAddNode(&loop, gph.loop_graph, &head, 1, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        int nlb = 0;
+        for (int part = 0; part < 4; ++part) nlb += enqueue_nr_part<T>(h, part, cs, A, pan, cb, cbr, x);
+        k_loop_cond<<<1, 1, 0, cs>>>(hc, h->any_active.as<int>(), d.it_ptr, max_it);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamEndCapture(cs, &body));
+        CUDA_TRY(cudaGraphInstantiate(&gph.loop_exec, gph.loop_graph, 0));
+        gph.loop_launches = nlb + 1;
       }
       CUDA_TRY(cudaStreamDestroy(cs));
       std::memcpy(gph.key, key, sizeof(key));
@@ -1852,7 +1898,17 @@ void solve_nr(mpf_handle* h, cudaStream_t st) {
       gph.ngroups = h->ngroups;
     }
   }
-  while (it < max_it && any_active(h, st)) {
+  if (dev_loop) {
+    // one launch for all iterations; their count is read back once
+    const int e = tm.begin(FAM_OTHER);
+    CUDA_TRY(cudaGraphLaunch(gph.loop_exec, st));
+    tm.end(e);
+    CUDA_TRY(cudaMemcpyAsync(h->h_any, d.it_ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    it = *h->h_any;
+    nl += 1 + it * gph.loop_launches;
+  }
+  while (!dev_loop && it < max_it && any_active(h, st)) {
     int e[4];
     for (int part = 0; part < 4; ++part) {
       e[part] = tm.begin(kFam[part]);

@@ -284,6 +284,15 @@ __global__ void k_init(DevGrid d, int ncases) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *d.it_ptr = 0;
 }
 
+// Condition of the device-side Newton loop (mpf_options.use_graph = 2), run before the
+// loop's while node and at the end of each body: another iteration while a case is
+// running and fewer than max_it iterations are done.  k_update_nr counts the
+// iterations in *it_ptr, so the loop stops after max_it bodies whatever the cases do.
+__global__ void k_loop_cond(cudaGraphConditionalHandle hc, const int* __restrict__ any_active,
+                            const int* __restrict__ it_ptr, int max_it) {
+  cudaGraphSetConditional(hc, (*any_active != 0 && *it_ptr < max_it) ? 1u : 0u);
+}
+
 // One thread per case (a warp = a group): decide convergence of the mismatch just
 // evaluated.  it = iterations done so far (it_arg, or the device counter when
 // it_arg < 0); the reference loop stops when max |F| < tol or it == max_it

@@ -202,11 +202,12 @@ def test_mismatch_entry_point_matches_solve_and_oracle(gpu):
 
 
 def test_graph_and_direct_launches_agree(gpu):
-    """The graph-captured iteration (default) and direct launches give identical
-    results, and replays after set_cases with a different batch size rebuild it."""
+    """The graph-captured iteration (default), the whole Newton loop as one graph with a
+    device-side while node (use_graph = 2) and direct launches give identical results,
+    and replays after set_cases with a different batch size rebuild the graphs."""
     buses, branches, cases = m.workload("cfg1_300bus")
     out = []
-    for use_graph in (1, 0):
+    for use_graph in (1, 0, 2):
         pf = m.PowerFlow(buses, branches)
         pf_opt = pf  # noqa: F841
         pf.close()
@@ -234,9 +235,47 @@ def test_graph_and_direct_launches_agree(gpu):
                 res.append((v.copy(), it.copy()))
         lib().mpf_destroy(h)
         out.append(res)
-    for (va, ia), (vb, ib) in zip(out[0], out[1]):
-        assert np.array_equal(ia, ib)
-        assert np.array_equal(va, vb)
+    for other in out[1:]:
+        for (va, ia), (vb, ib) in zip(out[0], other):
+            assert np.array_equal(ia, ib)
+            assert np.array_equal(va, vb)
+
+
+def test_device_loop_iteration_limit_and_q_limit_rounds(gpu):
+    """The device-side Newton loop stops at max_it_nr like the host loop (MAX_ITER per
+    case, same iteration counts) and runs again for each reactive-limit round."""
+    buses, branches, cases = m.workload("cfg1_300bus")
+    cases = [[]] + cases[:60]
+    rng = np.random.default_rng(5)
+    pv = np.where(buses["type"] == 2)[0]
+    qmin = np.full(len(buses), -np.inf)
+    qmax = np.full(len(buses), np.inf)
+    qmax[rng.choice(pv, len(pv) // 4, replace=False)] = 0.0
+    for max_it in (2, 10):
+        got = []
+        for use_graph in (1, 2):
+            with m.PowerFlow(buses, branches, use_graph=use_graph, max_it_nr=max_it) as pf:
+                if max_it == 10:
+                    pf.set_q_limits(qmin, qmax)  # before the cases: limits reset them
+                pf.set_cases(cases)
+                r = []
+                for prec in (m.FP64, m.MIXED):
+                    pf.solve(m.NR, prec)
+                    res = pf.results()
+                    r.append((res.status.copy(), res.iterations.copy(), res.v.copy(), pf.bus_types().copy()
+                              if max_it == 10 else None))
+                got.append(r)
+        for (sa, ia, va, ta), (sb, ib, vb, tb) in zip(*got):
+            assert np.array_equal(sa, sb) and np.array_equal(ia, ib) and np.array_equal(va, vb)
+            if ta is not None:
+                assert np.array_equal(ta, tb)
+        if max_it == 2:
+            from mapol_b200 import _types as T
+
+            assert (got[1][0][0] == T.CASE_MAX_ITER).any()
+        else:
+            # some cases switched PV buses to PQ (a second Newton run in the same solve)
+            assert ((got[1][0][3] == 1).sum(axis=1) > (buses["type"] == 1).sum()).any()
 
 
 def test_branch_flows_loss_and_overload_match_oracle(gpu):
