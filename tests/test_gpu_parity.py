@@ -79,6 +79,33 @@ def test_runpf_host_end_to_end(gpu):
     _compare(res, ref)
 
 
+def test_runpf_host_device_loop_equals_host_loop(gpu):
+    """mpf_runpf_host (case lists in from host memory, results out to host memory)
+    through the device-side Newton loop (use_graph = 2), as the bench's end-to-end figure
+    runs it, equals the host-read loop bit for bit, in both precisions."""
+    from mapol_b200._lib import lib, ptr
+    from mapol_b200.grid import cases_to_offsets
+
+    buses, branches, cases = m.workload("cfg1_300bus")
+    offs, flat = cases_to_offsets(cases)
+    n, nb = len(cases), len(buses)
+    out = {}
+    for use_graph in (1, 2):
+        with m.PowerFlow(buses, branches, use_graph=use_graph) as pf:
+            for prec in (m.MIXED, m.FP64):
+                v = np.zeros((n, nb, 2))
+                it = np.zeros(n, np.int32)
+                st = np.zeros(n, np.uint8)
+                mm = np.zeros(n)
+                assert lib().mpf_runpf_host(pf._h, m.NR, prec, n, ptr(offs), ptr(flat), None, ptr(v), ptr(it),
+                                            ptr(st), ptr(mm)) == 0
+                out[use_graph, prec] = (v, it, st, mm)
+    for prec in (m.MIXED, m.FP64):
+        assert (out[2, prec][2] == m.runpf.CONVERGED).sum() > 0.9 * n
+        for a, b in zip(out[1, prec], out[2, prec]):
+            assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("n_bus,n_branch,n_pv,n_out", [(118, 179, 53, 64), (1354, 1991, 259, 40)])
 def test_uneven_sizes_match_oracle(gpu, n_bus, n_branch, n_pv, n_out):
     buses, branches = m.synth_grid(n_bus, n_branch, n_pv, 0.1, seed=2)
