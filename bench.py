@@ -631,7 +631,8 @@ def run_multigrid(args, rank, world, local_rank):
     sampler = ClockSampler(local_rank) if rank == 0 else None
     if sampler:
         sampler.start()
-    with m.MultiGrid(grids, device=local_rank) as mg:
+    # both arms run the whole Newton loop as one CUDA graph (use_graph = 2)
+    with m.MultiGrid(grids, device=local_rank, use_graph=2) as mg:
         mg.set_cases(cases)
         for prec, name in ((m.MIXED, "mixed"), (m.FP64, "fp64")):
             ms = timed(lambda: mg.pf.solve(m.NR, prec, stream.cuda_stream))
@@ -640,7 +641,7 @@ def run_multigrid(args, rank, world, local_rank):
                              n_conv=int(sum((r.status == T.CASE_CONVERGED).sum() for r in res)))
     pfs = []
     for (b, br), cs in zip(grids, cases):
-        pf = m.PowerFlow(b, br, device=local_rank)
+        pf = m.PowerFlow(b, br, device=local_rank, use_graph=2)
         pf.set_cases(cs)
         pfs.append(pf)
 
@@ -664,7 +665,8 @@ def run_multigrid(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f64 mismatch/update/convergence test, f32 LU factorisation and solves",
         "data": "synthetic (seeded generator)",
         "config": {"workload": args.workload, "grids": WORKLOAD_SETS[args.workload],
-                   "cases_per_grid": [len(c) for c in cases], "alg": "NR"},
+                   "cases_per_grid": [len(c) for c in cases], "alg": "NR",
+                   "newton_loop": "one CUDA graph per solve (use_graph = 2)"},
         "plain_fp64": {"value": n_cases * world * args.steps / (out["fp64"]["ms"] / 1e3),
                        "ms_per_step": out["fp64"]["ms"] / args.steps},
         "converged": {"mixed": out["mixed"]["n_conv"], "fp64": out["fp64"]["n_conv"], "of": n_cases},

@@ -134,3 +134,22 @@ def test_island_inputs_are_checked(gpu):
     br3["to"] += len(b1)
     with pytest.raises(m.MpfError):
         m.PowerFlow(np.concatenate([b1, b3]), np.concatenate([br1, br3]))
+
+
+def test_device_loop_equals_host_loop(cfg2):
+    """The whole Newton loop as one CUDA graph (use_graph = 2, as the config-2 bench runs
+    it) gives each grid of the batch the host-read loop's results bit for bit."""
+    grids, cases = cfg2
+    out = []
+    for use_graph in (1, 2):
+        with m.MultiGrid(grids, use_graph=use_graph) as mg:
+            mg.set_cases(cases)
+            r = []
+            for prec in (m.FP64, m.MIXED):
+                mg.solve(m.NR, prec)
+                r.append([(x.v.copy(), x.iterations.copy(), x.status.copy()) for x in mg.results()])
+            out.append(r)
+    for pa, pb in zip(*out):
+        for ga, gb in zip(pa, pb):
+            for a, b in zip(ga, gb):
+                assert np.array_equal(a, b)
