@@ -60,7 +60,8 @@ def profile_solve(args):
     if args.cases:
         cases = cases[:args.cases]
     prec = m.MIXED if args.profile_solve == "mixed" else m.FP64
-    with m.PowerFlow(buses, branches) as pf:
+    # the host-read Newton loop, whose timing splits the solve by kernel family
+    with m.PowerFlow(buses, branches, use_graph=1) as pf:
         pf.set_cases(cases)
         for _ in range(max(1, args.warmup)):
             pf.solve(m.NR, prec)
@@ -389,7 +390,7 @@ def run_ours(args, rank, world, local_rank):
         cases = cases[: args.cases]
     n_cases = len(cases)
     t_create = time.perf_counter()
-    pf = m.PowerFlow(buses, branches, device=local_rank)
+    pf = m.PowerFlow(buses, branches, device=local_rank, use_graph=1)  # per-family kernel times
     t_create = time.perf_counter() - t_create
     pf.set_cases(cases)
     stream = torch.cuda.current_stream()

@@ -113,11 +113,13 @@ typedef struct mpf_options {
   int32_t angle_mode;  /* 0: atan2 (default); 1: atan(y/x) as cuCangle in
                           src/util/complexUtils.h:21-23 (loses the quadrant) */
   int32_t device;      /* CUDA device ordinal, default 0 */
-  int32_t use_graph;   /* 1: capture the Newton iteration in CUDA graphs, the host reads
-                          one flag per iteration (default 1); 2: the whole Newton loop as
-                          one CUDA graph whose while node tests the flag and the iteration
-                          count on the device (one read-back per solve; mpf_timing then
-                          reports the loop in other_ms); 0: direct launches */
+  int32_t use_graph;   /* 2: the whole Newton loop as one CUDA graph whose while node
+                          tests "any case running" and the iteration count on the device
+                          (one read-back per solve; mpf_timing then reports the loop in
+                          other_ms) (default 2); 1: the Newton iteration as captured CUDA
+                          graphs, the host reads one flag per iteration and mpf_timing
+                          splits the solve by kernel family; 0: direct launches.  All
+                          three give the same results bit for bit. */
   int32_t autotune;    /* 1: time the candidate kernels of every factorisation launch on
                           the first solve of a batch size and keep the fastest (default 1);
                           0: fixed heuristic */

@@ -2207,7 +2207,7 @@ void mpf_default_options(mpf_options* opt) {
   opt->tol = MPF_DEFAULT_TOL;
   opt->angle_mode = 0;
   opt->device = 0;
-  opt->use_graph = 1;
+  opt->use_graph = 2;
   opt->autotune = 1;
 }
 

@@ -45,7 +45,7 @@ class PowerFlow:
     """One grid on one GPU (mpf_create).  Replaces hybrid_init / hybrid_free."""
 
     def __init__(self, buses, branches, max_it_nr=MAX_IT_NR, max_it_fd=MAX_IT_FD, tol=EPS,
-                 angle_mode=0, device=0, use_graph=1, autotune=1, ordering=T.ORDER_AUTO):
+                 angle_mode=0, device=0, use_graph=2, autotune=1, ordering=T.ORDER_AUTO):
         self.buses = np.ascontiguousarray(buses, dtype=T.BUS_DTYPE)
         self.branches = np.ascontiguousarray(branches, dtype=T.BRANCH_DTYPE)
         opt = T.Options()
